@@ -1,0 +1,836 @@
+"""Fitting: BMC-JAX's `bmc_jax.fitting` API on the B200 kernels.
+
+  FreeParam, FitSpec, write_params   which parameters are free    (fitting/params.py:38-112)
+  Experiment                         what is simulated            (fitting/experiment.py:21-141)
+  levenberg_marquardt                bounded LM, physics-free     (fitting/lm.py:20-67)
+  fit, fit_batch                     every sample alone           (fitting/independent.py:51-129, 226-298)
+  fit_joint                          shared / per-block / partly free values (fitting/joint.py:165-453)
+  FitResult                          what comes back              (fitting/result.py:23-174)
+
+`fit` and `fit_batch` run every LM iteration of every voxel on the GPU (bmc_lm_fit): residual,
+forward-mode Jacobian, float64 normal equations, damped solve, clip, trial residual, accept/reject.
+`fit_joint` without a shared or per-block value is the same device loop with per-sample holds; with
+one, the samples are coupled and one damping governs the joint step: the host loop of the reference
+(joint.py:375-416) with per-sample Jacobians from the GPU and the joint normal equations solved by a
+Schur complement over the shared columns (the same linear system as the reference's dense solve).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib
+from .simulation import (SimParams, SimEvent, EventType, pad_events, tile_params, n_cest_of, n_samples,
+                         pack_params, state_size, DeviceEvents, problem, initial_state, B0Spread, _device)
+
+__all__ = ["Experiment", "FreeParam", "FitSpec", "write_params", "levenberg_marquardt", "fit", "fit_batch",
+           "fit_joint", "FitResult"]
+
+PSEUDO = ("m_start", "b0_spread")
+_SCALAR_FIELDS = ("water_r1", "water_r2", "water_f", "mt_k", "mt_f", "mt_dw", "mt_r1", "mt_r2", "mt_lineshape",
+                  "b0", "gamma", "b0_inhom", "rel_b1")
+_POOL_FIELDS = ("cest_k", "cest_f", "cest_dw", "cest_r1", "cest_r2")
+
+
+def field_row(field: str, index: Optional[int], n_cest: int) -> int:
+    """Row of a SimParams field value in the C ABI's params layout."""
+    if field in _POOL_FIELDS:
+        if index is None or not 0 <= int(index) < n_cest:
+            raise ValueError(f"{field}: pool index {index} outside 0..{n_cest - 1}")
+        return 3 + _POOL_FIELDS.index(field) * n_cest + int(index)
+    if field in ("water_r1", "water_r2", "water_f"):
+        return ("water_r1", "water_r2", "water_f").index(field)
+    if field in _SCALAR_FIELDS:
+        return 3 + 5 * n_cest + _SCALAR_FIELDS[3:].index(field)
+    raise ValueError(f"{field}: not a SimParams field")
+
+
+# ------------------------------------------------------------------------------------------------
+# which parameters are free (fitting/params.py)
+# ------------------------------------------------------------------------------------------------
+@dataclass(frozen=True)
+class FreeParam:
+    name: str
+    field: str
+    index: Optional[int]
+    scale: float
+    lo: float
+    hi: float
+    x0: float
+    scope: str = "sample"
+    samples: Optional[Tuple[int, ...]] = None
+    mode: str = "value"
+
+    def __post_init__(self):
+        if self.scope not in ("sample", "shared", "block"):
+            raise ValueError(f"{self.name}: scope {self.scope!r}; use 'sample', 'shared' or 'block'")
+        if self.mode not in ("value", "factor", "add"):
+            raise ValueError(f"{self.name}: mode {self.mode!r}; use 'value', 'factor' or 'add'")
+        if self.field == "m_start" and (self.index is not None or self.mode == "add"):
+            raise ValueError(f"{self.name}: m_start is one number per sample (index None), as a value or a factor")
+        if self.field == "b0_spread" and (self.index is not None or self.mode != "value"):
+            raise ValueError(f"{self.name}: b0_spread is one width in Hz (index None, mode 'value')")
+        if self.samples is not None:
+            object.__setattr__(self, "samples", tuple(sorted({int(i) for i in self.samples})))
+            if not self.samples:
+                raise ValueError(f"{self.name}: samples=() frees it nowhere; leave it out of the spec")
+
+
+@dataclass(frozen=True)
+class FitSpec:
+    slots: List[FreeParam]
+
+    @property
+    def n(self):
+        return len(self.slots)
+
+    @property
+    def scales(self):
+        return np.array([s.scale for s in self.slots], np.float64)
+
+    @property
+    def lo_phys(self):
+        return np.array([s.lo for s in self.slots], np.float64)
+
+    @property
+    def hi_phys(self):
+        return np.array([s.hi for s in self.slots], np.float64)
+
+    @property
+    def x0_phys(self):
+        return np.array([s.x0 for s in self.slots], np.float64)
+
+    def to_scaled(self, x_phys):
+        return np.asarray(x_phys) / self.scales
+
+    def to_phys(self, x_scaled):
+        return np.asarray(x_scaled) * self.scales
+
+    @property
+    def independent(self) -> bool:
+        return all(s.scope == "sample" and s.samples is None and s.mode == "value" and s.field not in PSEUDO
+                   for s in self.slots)
+
+    def require_independent(self, caller: str) -> None:
+        if not self.independent:
+            joint = [s.name for s in self.slots if s.scope != "sample" or s.samples is not None
+                     or s.mode != "value" or s.field in PSEUDO]
+            raise ValueError(f"{caller}: {joint} are shared, per block, free in some samples only, a factor / an "
+                             "offset, m_start or b0_spread (FreeParam scope / samples / mode / field), which "
+                             "samples fitted alone with plain values cannot do; use fit_joint")
+
+
+def write_params(base: SimParams, x_scaled, spec: FitSpec) -> SimParams:
+    """Scaled x -> physical values written into the named fields (fitting/params.py:100-112)."""
+    x_phys = np.asarray(x_scaled, np.float64) * spec.scales
+    upd = {}
+    for i, s in enumerate(spec.slots):
+        if s.index is None:
+            upd[s.field] = x_phys[..., i]
+        else:
+            cur = np.array(upd.get(s.field, getattr(base, s.field)), np.float64, copy=True)
+            cur[..., s.index] = x_phys[..., i]
+            upd[s.field] = cur
+    return base._replace(**upd)
+
+
+# ------------------------------------------------------------------------------------------------
+# what is simulated (fitting/experiment.py)
+# ------------------------------------------------------------------------------------------------
+@dataclass(frozen=True)
+class Experiment:
+    """Parameters, a sequence, a starting state, and the index of water's Mz."""
+    params: object
+    events: SimEvent
+    m0: object
+    mz_loc: int
+
+    @property
+    def n_offsets(self) -> int:
+        return int(np.shape(self.events.dt)[0])
+
+    @property
+    def n_events(self) -> int:
+        return int(np.shape(self.events.dt)[1])
+
+    def simulate(self) -> np.ndarray:
+        """Water Mz at every offset: (n_offsets,) for one sample, (n_samples, n_offsets) for a batch."""
+        from .simulation import simulate_z
+        return simulate_z(self.params, self.events, self.m0, self.mz_loc)
+
+    @classmethod
+    def from_parameters(cls, params, events) -> "Experiment":
+        from .simulation import to_sim_params
+        jp = to_sim_params(params)
+        scale = float(getattr(params.options, "scale", 1.0))
+        return cls(jp, events, initial_state(jp, scale), params.mz_loc)
+
+    @classmethod
+    def stack(cls, experiments: Sequence["Experiment"]) -> "Experiment":
+        experiments = list(experiments)
+        if not experiments:
+            raise ValueError("stack needs at least one experiment")
+        locs = {p.mz_loc for p in experiments}
+        if len(locs) > 1:
+            raise ValueError(f"experiments disagree on mz_loc: {sorted(locs)}; they must describe "
+                             "the same pools in the same order")
+        width = max(p.n_events for p in experiments)
+        padded = [pad_events(p.events, width) for p in experiments]
+        events = SimEvent(*[np.concatenate([np.asarray(getattr(e, f)) for e in padded], axis=0)
+                            for f in SimEvent._fields])
+        first = experiments[0]
+        return cls(first.params, events, first.m0, first.mz_loc)
+
+
+# ------------------------------------------------------------------------------------------------
+# what comes back (fitting/result.py)
+# ------------------------------------------------------------------------------------------------
+@dataclass(frozen=True)
+class FitResult:
+    x: np.ndarray
+    z_fit: np.ndarray
+    z_meas: np.ndarray
+    spec: FitSpec
+    n_per_block: Optional[int] = None
+    free: Optional[np.ndarray] = None
+    sd: Optional[np.ndarray] = None
+    corr: Optional[np.ndarray] = None
+    x0: Optional[np.ndarray] = None
+    cost: Optional[np.ndarray] = None
+    nan_steps: int = 0
+    blocks: Optional[dict] = None
+
+    @property
+    def names(self) -> List[str]:
+        return [s.name for s in self.spec.slots]
+
+    def __getitem__(self, name: str) -> np.ndarray:
+        if self.blocks and name in self.blocks:
+            return self.blocks[name]["x"]
+        try:
+            return self.x[:, self.names.index(name)]
+        except ValueError:
+            raise KeyError(f"no parameter {name!r}; the fit has {self.names}") from None
+
+    @property
+    def residual(self) -> np.ndarray:
+        return self.z_fit - self.z_meas
+
+    @property
+    def rms(self) -> np.ndarray:
+        return np.sqrt(np.mean(self.residual ** 2, axis=-1))
+
+    @property
+    def rms_per_block(self):
+        if self.n_per_block is None:
+            return None
+        nb = self.z_meas.shape[-1] // self.n_per_block
+        r = self.residual[..., :nb * self.n_per_block]
+        return np.sqrt(np.mean(r.reshape(*r.shape[:-1], nb, self.n_per_block) ** 2, axis=-1))
+
+    @property
+    def at_bounds(self) -> np.ndarray:
+        lo, hi = np.asarray(self.spec.lo_phys), np.asarray(self.spec.hi_phys)
+        railed = np.isclose(self.x, lo) | np.isclose(self.x, hi)
+        return railed if self.free is None else railed & self.free
+
+    @property
+    def unmoved(self):
+        if self.x0 is None:
+            return None
+        still = np.isclose(self.x, self.x0, rtol=1e-6, atol=0.0)
+        return still if self.free is None else still & self.free
+
+    def summary(self) -> str:
+        head = f"{'sample':>6}  " + "  ".join(f"{n:>12}" for n in self.names) + f"  {'rms':>9}"
+        rows = [head, "-" * len(head)]
+        ab = self.at_bounds
+        for i in range(self.x.shape[0]):
+            cells = []
+            for j, _ in enumerate(self.names):
+                mark = "*" if ab[i, j] else ("=" if self.free is not None and not self.free[i, j] else " ")
+                cells.append(f"{self.x[i, j]:>11.5g}{mark}")
+            rows.append(f"{i:>6}  " + "  ".join(cells) + f"  {self.rms[i]:>9.2e}")
+        if ab.any():
+            rows.append("* on a bound -- not a measurement, the optimiser was stopped there")
+        if self.free is not None and not self.free.all():
+            rows.append("= not free in this sample: the value its params carry")
+        for name, b in (self.blocks or {}).items():
+            rows.append(f"{name} per experiment: " + "  ".join(
+                f"{v:.5g}{'*' if r else ''}" for v, r in zip(b["x"], b["at_bounds"])))
+        return "\n".join(rows)
+
+    def __repr__(self) -> str:
+        railed = int(self.at_bounds.sum())
+        return (f"FitResult({self.x.shape[0]} samples, {self.names}, "
+                f"rms {self.rms.mean():.3e}" + (f", {railed} at bounds)" if railed else ")"))
+
+
+# ------------------------------------------------------------------------------------------------
+# bounded LM without physics (fitting/lm.py:20-67), for any residual function on the host
+# ------------------------------------------------------------------------------------------------
+def levenberg_marquardt(resid_fn, x0, lo, hi, n_iter=40, lam0=1e-2, use_fwd=False, return_trajectory=False,
+                        free=None, jac_fn=None):
+    """Damped Gauss-Newton for one residual vector, fixed iterations with accept/reject, float64.
+
+    The step rule is the reference's exactly. `jac_fn(x)` gives the Jacobian; without it a central
+    difference is used (this entry point is physics-free: the BMC fits use the GPU's exact tangents)."""
+    x = np.asarray(x0, np.float64).copy()
+    lo, hi = np.asarray(lo, np.float64), np.asarray(hi, np.float64)
+    P = x.size
+    fr = None if free is None else np.asarray(free, np.float64)
+
+    def jac(x):
+        if jac_fn is not None:
+            return np.asarray(jac_fn(x), np.float64)
+        r0 = np.asarray(resid_fn(x), np.float64)
+        J = np.empty((r0.size, P))
+        for j in range(P):
+            h = 1e-7 * max(1.0, abs(x[j]))
+            e = np.zeros(P)
+            e[j] = h
+            J[:, j] = (np.asarray(resid_fn(x + e)) - np.asarray(resid_fn(x - e))) / (2 * h)
+        return J
+
+    lam = float(lam0)
+    X, Cs = [], []
+    for _ in range(n_iter):
+        r = np.asarray(resid_fn(x), np.float64)
+        c = float(r @ r)
+        J = jac(x)
+        if fr is not None:
+            J = J * fr
+        g, H = J.T @ r, J.T @ J
+        A = H + lam * (np.diag(np.diag(H)) + 1e-9 * np.eye(P))
+        if fr is not None:
+            A = A + np.diag(1.0 - fr)
+        xn = np.clip(x + np.linalg.solve(A, -g), lo, hi)
+        rn = np.asarray(resid_fn(xn), np.float64)
+        cn = float(rn @ rn)
+        better = cn < c
+        x = xn if better else x
+        lam = lam * 0.5 if better else lam * 3.0
+        X.append(x.copy())
+        Cs.append(cn if better else c)
+    if return_trajectory:
+        return x, np.array(X), np.array(Cs)
+    return x
+
+
+# ------------------------------------------------------------------------------------------------
+# the device LM (bmc_lm_fit)
+# ------------------------------------------------------------------------------------------------
+def _lm_device(params_b: SimParams, events: SimEvent, m0_b, mz: int, rows, modes, scales, lo, hi, z_meas, X0,
+               n_iter: int, lam0: float, skip: int = 0, free=None, spread=None, sigma=None):
+    """Run bmc_lm_fit; returns (x scaled (n, P), cost trajectory (n, n_iter))."""
+    torch = _lib.torch_cuda()
+    n = n_samples(params_b)
+    nc = n_cest_of(params_b)
+    N = state_size(nc)
+    P = len(rows)
+    if P > _lib.MAX_TANGENTS:
+        raise ValueError(f"at most {_lib.MAX_TANGENTS} free parameters per sample, got {P}")
+    dev_ev = DeviceEvents(events)
+    pdev = _device(pack_params(params_b, n))
+    mdev = _device(np.broadcast_to(np.asarray(m0_b, np.float64), (n, N)))
+    zdev = _device(z_meas)
+    xdev = _device(X0)
+    fdev = None if free is None else _device(np.asarray(free, np.float64))
+    xout = torch.empty((n, P), dtype=torch.float64, device="cuda")
+    ctraj = torch.empty((n, max(n_iter, 1)), dtype=torch.float64, device="cuda")
+    spec = _lib.FitSpecC()
+    spec.n_params, spec.n_iter, spec.lam0 = P, int(n_iter), float(lam0)
+    for p in range(P):
+        spec.field_row[p], spec.mode[p] = int(rows[p]), int(modes[p])
+        spec.scale[p], spec.lo[p], spec.hi[p] = float(scales[p]), float(lo[p]), float(hi[p])
+    spec.d_free = None if fdev is None else fdev.data_ptr()
+    spec.n_points_skip = int(skip)
+    sp, keep = (None, None)
+    if spread is not None:
+        u, w = spread.nodes_weights()
+        sdev = _device(np.broadcast_to(np.asarray(sigma, np.float64), (n,)))
+        sp, keep = _lib.spread_struct(u, w, sdev)
+    pr = problem(n, dev_ev.n_offsets, dev_ev.n_events, nc, int(mz), _lib.F64)
+    _lib.check(_lib.lib().bmc_lm_fit(pr, _lib.ptr(pdev), dev_ev.struct, _lib.ptr(mdev), sp, spec, _lib.ptr(zdev),
+                                     _lib.ptr(xdev), _lib.ptr(xout), _lib.ptr(ctraj), None, _lib.stream_handle()))
+    x = xout.cpu().numpy()
+    c = ctraj.cpu().numpy()[:, :n_iter]
+    del keep
+    return x, c
+
+
+def _slot_rows(spec: FitSpec, nc: int):
+    rows, modes = [], []
+    for s in spec.slots:
+        if s.field == "m_start":
+            rows.append(_lib.SLOT_M_START)
+        elif s.field == "b0_spread":
+            rows.append(_lib.SLOT_SPREAD_SIGMA)
+        else:
+            rows.append(field_row(s.field, s.index, nc))
+        modes.append({"value": 0, "factor": 1, "add": 2}[s.mode])
+    return rows, modes
+
+
+def _batched(params, n):
+    return params if n_samples(params) is not None else tile_params(params, n)
+
+
+def fit_batch(base, events, M0_batch, water_z, spec: FitSpec, z_meas_batch, X0_phys=None, n_iter=40,
+              skip_first=True, base_batched=False, use_fwd=None, max_chunk=None, dtype=None):
+    """Every voxel with damped Gauss-Newton, all on the GPU (independent.py:51-129). Returns physical
+    X (n, P). The Jacobian is always forward mode (use_fwd is accepted for compatibility); `dtype`
+    is accepted and ignored: fits run in float64."""
+    spec.require_independent("fit_batch")
+    z = np.asarray(z_meas_batch, np.float64)
+    n_vox = z.shape[0]
+    base_b = base if base_batched else tile_params(base, n_vox)
+    nc = n_cest_of(base_b)
+    N = state_size(nc)
+    M0_b = np.asarray(M0_batch, np.float64)
+    if M0_b.ndim == 1:
+        M0_b = np.broadcast_to(M0_b, (n_vox,) + M0_b.shape)
+    if M0_b.shape[0] != n_vox:
+        raise ValueError(f"M0_batch has {M0_b.shape[0]} rows for {n_vox} voxels")
+    skip = 1 if skip_first else 0
+    z_t = z[:, skip:]
+    scales = spec.scales
+    lo, hi = spec.lo_phys / scales, spec.hi_phys / scales
+    X0 = (np.broadcast_to(spec.to_scaled(spec.x0_phys), (n_vox, spec.n)) if X0_phys is None
+          else np.broadcast_to(spec.to_scaled(X0_phys), (n_vox, spec.n)))
+    rows, modes = _slot_rows(spec, nc)
+    chunk = max_chunk or n_vox
+    parts = []
+    for a in range(0, n_vox, chunk):
+        b = min(a + chunk, n_vox)
+        sub = SimParams(*[np.asarray(v)[a:b] for v in base_b])
+        x, _ = _lm_device(sub, events, M0_b[a:b], water_z, rows, modes, scales, lo, hi, z_t[a:b], X0[a:b],
+                          n_iter, 1e-2, skip)
+        parts.append(x)
+    return np.concatenate(parts) * scales
+
+
+def fit(experiment: Experiment, spec: FitSpec, z_meas, n_iter=30, x0_phys=None, n_per_block=None, **kwargs):
+    """Fit `spec`'s parameters of `experiment` to `z_meas` (independent.py:226-298)."""
+    from .simulation import simulate_z
+    spec.require_independent("fit")
+    z = np.atleast_2d(np.asarray(z_meas, np.float64))
+    n = z.shape[0]
+    base = _batched(experiment.params, n)
+    m0 = np.asarray(experiment.m0, np.float64)
+    if m0.ndim == 1:
+        m0 = np.broadcast_to(m0, (n,) + m0.shape)
+    X = fit_batch(base, experiment.events, m0, experiment.mz_loc, spec, z, X0_phys=x0_phys, n_iter=n_iter,
+                  skip_first=False, base_batched=True, **kwargs)
+    z_fit = simulate_z(write_params(base, spec.to_scaled(X), spec), experiment.events, m0, experiment.mz_loc,
+                       precision=_lib.F64)
+    return FitResult(X, np.asarray(z_fit), z, spec, n_per_block)
+
+
+# ------------------------------------------------------------------------------------------------
+# joint fits (fitting/joint.py)
+# ------------------------------------------------------------------------------------------------
+def _layout(spec: FitSpec, n: int, n_blocks: int):
+    """free (n, L); pos (L,); n_loc; cols [(slot, samples, block or -1)] per joint column."""
+    width = [n_blocks if s.scope == "block" else 1 for s in spec.slots]
+    pos = np.concatenate([[0], np.cumsum(width)[:-1]]).astype(int)
+    free = np.zeros((n, spec.n), bool)
+    cols = []
+    for l, s in enumerate(spec.slots):
+        who = list(range(n)) if s.samples is None else list(s.samples)
+        missing = [i for i in who if not 0 <= i < n]
+        if missing:
+            raise ValueError(f"{s.name}: samples {missing} do not exist (the fit has {n})")
+        free[who, l] = True
+        if s.scope == "shared":
+            cols.append((l, who, -1))
+        elif s.scope == "block":
+            cols += [(l, who, b) for b in range(n_blocks)]
+        else:
+            cols += [(l, [i], -1) for i in who]
+    return free, pos, int(sum(width)), cols
+
+
+def _carried(params: SimParams, m0, spec: FitSpec, sig_held):
+    """(n, L): each slot's number where it is not free (joint.py:99-117)."""
+    n = m0.shape[0]
+    nc = n_cest_of(params)
+    out = []
+    for s in spec.slots:
+        if s.field == "b0_spread":
+            out.append(np.asarray(sig_held, np.float64))
+        elif s.mode == "factor":
+            out.append(np.ones(n))
+        elif s.mode == "add":
+            out.append(np.zeros(n))
+        elif s.field == "m_start":
+            out.append(m0[:, 2 * (1 + nc)] / np.asarray(params.water_f, np.float64))
+        else:
+            a = np.asarray(getattr(params, s.field), np.float64)
+            out.append(a if s.index is None else a[:, s.index])
+    return np.stack(out, axis=1)
+
+
+class _JointModel:
+    """Per-sample model and local Jacobian of a joint fit on the GPU (joint.py:289-348)."""
+
+    def __init__(self, params, m0, events, mz, spec, free, pos, n_loc, nb, n_per_block, spread, sig_held):
+        self.params, self.m0, self.mz, self.spec = params, m0, mz, spec
+        self.free, self.pos, self.n_loc, self.nb = free, pos, n_loc, nb
+        self.spread, self.sig_held = spread, sig_held
+        self.n = m0.shape[0]
+        self.nc = n_cest_of(params)
+        self.N = state_size(self.nc)
+        self.is_block = np.array([s.scope == "block" for s in spec.slots])
+        n_off = np.shape(events.dt)[0]
+        self.n_pts = n_off
+        if nb > 1:
+            self.blocks = [SimEvent(*[np.asarray(a)[b * n_per_block:(b + 1) * n_per_block] for a in events])
+                           for b in range(nb)]
+        else:
+            self.blocks = [events]
+        self.dev_blocks = [DeviceEvents(e) for e in self.blocks]
+        self.rows, _ = _slot_rows(spec, self.nc)
+        self.mslot = next((l for l, s in enumerate(spec.slots) if s.field == "m_start"), None)
+        self.sslot = next((l for l, s in enumerate(spec.slots) if s.field == "b0_spread"), None)
+
+    def _effective(self, loc, b):
+        """Per-sample params, start state, width and field seeds for block b (joint.py:120-138)."""
+        spec = self.spec
+        L = spec.n
+        eff = np.where(self.free, loc[:, [self.pos[l] + (b if self.is_block[l] else 0) for l in range(L)]] *
+                       spec.scales, self.carried_in[:, :L])
+        upd = {}
+        seeds = np.zeros((L, self.n))
+        for l, s in enumerate(spec.slots):
+            if s.field in PSEUDO:
+                continue
+            cur = np.array(upd.get(s.field, np.asarray(getattr(self.params, s.field), np.float64)), copy=True)
+            old = cur if s.index is None else cur[:, s.index]
+            new = eff[:, l] if s.mode == "value" else (old * eff[:, l] if s.mode == "factor" else old + eff[:, l])
+            seeds[l] = np.where(self.free[:, l], s.scale * (old if s.mode == "factor" else 1.0), 0.0)
+            if s.index is None:
+                cur = new
+            else:
+                cur[:, s.index] = new
+            upd[s.field] = cur
+        q = self.params._replace(**upd)
+        m = self.m0.copy()
+        dm0 = np.zeros((L, self.n, self.N))
+        if self.mslot is not None:
+            ms = spec.slots[self.mslot]
+            mv = eff[:, self.mslot]
+            fr = self.free[:, self.mslot]
+            ist = np.stack([initial_state(SimParams(*[np.asarray(v)[i] for v in q])) for i in range(self.n)])
+            rebuilt = ist * mv[:, None] if ms.mode == "value" else self.m0 * mv[:, None]
+            m = np.where(fr[:, None], rebuilt, self.m0)
+            base_m = ist if ms.mode == "value" else self.m0
+            dm0[self.mslot] = np.where(fr[:, None], base_m * ms.scale, 0.0)
+            if ms.mode == "value":                     # the rebuilt state follows the pools' f
+                nc = self.nc
+                for l, s in enumerate(spec.slots):
+                    if s.field in ("water_f", "cest_f", "mt_f"):
+                        qi = {"water_f": 2 * (1 + nc), "mt_f": 3 * (1 + nc)}.get(s.field)
+                        if s.field == "cest_f":
+                            qi = 2 * (1 + nc) + 1 + int(s.index)
+                        dm0[l, :, qi] += np.where(fr, mv * seeds[l], 0.0)
+        sig = self.sig_held
+        if self.sslot is not None:
+            sig = np.where(self.free[:, self.sslot], eff[:, self.sslot], self.sig_held)
+            seeds[self.sslot] = np.where(self.free[:, self.sslot], spec.slots[self.sslot].scale, 0.0)
+        return q, m, sig, seeds, dm0
+
+    def evaluate(self, loc, need_jac=True):
+        """Z (n, n_pts) and, with need_jac, the local Jacobian (n, n_pts, n_loc)."""
+        torch = _lib.torch_cuda()
+        L = self.spec.n
+        Z = np.empty((self.n, self.n_pts))
+        J = np.zeros((self.n, self.n_pts, self.n_loc)) if need_jac else None
+        for b, dev_ev in enumerate(self.dev_blocks):
+            q, m, sig, seeds, dm0 = self._effective(loc, b)
+            rows = slice(b * dev_ev.n_offsets, (b + 1) * dev_ev.n_offsets)
+            pdev = _device(pack_params(q, self.n))
+            mdev = _device(m)
+            pr = problem(self.n, dev_ev.n_offsets, dev_ev.n_events, self.nc, int(self.mz), _lib.F64)
+            sp, keep = (None, None)
+            if self.spread is not None:
+                u, w = self.spread.nodes_weights()
+                sdev = _device(np.broadcast_to(np.asarray(sig, np.float64), (self.n,)))
+                sp, keep = _lib.spread_struct(u, w, sdev)
+            z = torch.empty((self.n, dev_ev.n_offsets), dtype=torch.float64, device="cuda")
+            if need_jac:
+                jz = torch.empty((L, self.n, dev_ev.n_offsets), dtype=torch.float64, device="cuda")
+                tg = _lib.Tangents()
+                tg.n_tangents = L
+                for l in range(L):
+                    tg.field_row[l] = (_lib.SEED_NONE if self.rows[l] == _lib.SLOT_M_START else self.rows[l])
+                sdev_seed = _device(seeds)
+                ddm0 = _device(dm0) if self.mslot is not None else None
+                tg.d_seed = sdev_seed.data_ptr()
+                tg.d_dm0 = None if ddm0 is None else ddm0.data_ptr()
+                _lib.check(_lib.lib().bmc_simulate_jvp(pr, _lib.ptr(pdev), dev_ev.struct, _lib.ptr(mdev), sp, tg,
+                                                       _lib.ptr(z), _lib.ptr(jz), _lib.stream_handle()))
+                jl = jz.cpu().numpy()
+                for l in range(L):
+                    J[:, rows, self.pos[l] + (b if self.is_block[l] else 0)] = jl[l]
+            else:
+                _lib.check(_lib.lib().bmc_simulate(pr, _lib.ptr(pdev), dev_ev.struct, _lib.ptr(mdev), sp,
+                                                   _lib.ptr(z), _lib.stream_handle()))
+            Z[:, rows] = z.cpu().numpy()
+            del keep
+        return Z, J
+
+
+def _joint_solve(Hl, gl, col_of, shared, P, lam, keep=None):
+    """Solve (H + lam (diag H + 1e-9 I)) d = -g for the joint columns, H = sum_i G_i^T Hl_i G_i.
+
+    `col_of[i]` maps sample i's local entries to joint columns (-1 = not a column). Columns used by
+    one sample only are eliminated per sample (block diagonal); the `shared` columns by the Schur
+    complement. The same linear system as joint.py:149-162's dense solve."""
+    n = Hl.shape[0]
+    shared = np.asarray(sorted(shared), int)
+    S = shared.size
+    sidx = {c: k for k, c in enumerate(shared)}
+    H_ss = np.zeros((S, S))
+    g_s = np.zeros(S)
+    blocks = []
+    # diagonal of the full H first (the damping uses it)
+    diag = np.zeros(P)
+    g = np.zeros(P)
+    for i in range(n):
+        cols = col_of[i]
+        use = np.flatnonzero(cols >= 0)
+        c = cols[use]
+        np.add.at(diag, c, np.diag(Hl[i])[use])
+        np.add.at(g, c, gl[i][use])
+    if keep is not None:
+        g = g * keep
+    for i in range(n):
+        cols = col_of[i]
+        use = np.flatnonzero(cols >= 0)
+        c = cols[use]
+        Hi = Hl[i][np.ix_(use, use)]
+        priv = np.array([cc not in sidx for cc in c], bool)
+        blocks.append((c, Hi, priv))
+    # assemble: private block per sample, coupling to shared, shared block
+    sol = np.zeros(P)
+    Ainv_data = []
+    for i, (c, Hi, priv) in enumerate(blocks):
+        ks = keep[c] if keep is not None else np.ones(c.size)
+        Hi = Hi * ks[:, None] * ks[None, :]
+        cp, cs = c[priv], c[~priv]
+        App = Hi[np.ix_(priv, priv)] + lam * np.diag(diag[cp] * (ks[priv] if keep is not None else 1.0) + 1e-9)
+        if keep is not None:
+            App = App + np.diag(1.0 - ks[priv]) * (1.0 + lam)
+        Aps = Hi[np.ix_(priv, ~priv)]
+        si = np.array([sidx[x] for x in cs], int)
+        if S:
+            np.add.at(H_ss, np.ix_(si, si), Hi[np.ix_(~priv, ~priv)])
+        if cp.size:
+            Y = np.linalg.solve(App, np.concatenate([Aps, -g[cp][:, None]], axis=1)) if cp.size else None
+            Ainv_data.append((cp, si, App, Aps, Y))
+            if S and si.size:
+                np.add.at(H_ss, np.ix_(si, si), -Aps.T @ Y[:, :-1])
+                np.add.at(g_s, si, -(Aps.T @ Y[:, -1]))
+        else:
+            Ainv_data.append((cp, si, None, None, None))
+    if S:
+        ks = keep[shared] if keep is not None else np.ones(S)
+        Ass = H_ss + lam * np.diag(diag[shared] * ks + 1e-9)
+        if keep is not None:
+            Ass = Ass + np.diag(1.0 - ks) * (1.0 + lam)
+        ds = np.linalg.solve(Ass, -g[shared] + g_s)
+        sol[shared] = ds
+    for cp, si, App, Aps, Y in Ainv_data:
+        if cp.size:
+            rhs = -g[cp] - (Aps @ sol[shared[si]] if (S and si.size) else 0.0)
+            sol[cp] = np.linalg.solve(App, rhs)
+    return sol
+
+
+def _cov_to_sd_corr(cov, scale):
+    sd = np.sqrt(np.clip(np.diag(cov), 0.0, None))
+    with np.errstate(invalid="ignore", divide="ignore"):
+        corr = cov / np.outer(sd, sd)
+    return sd * scale, corr
+
+
+def fit_joint(experiment: Experiment, spec: FitSpec, z_meas, n_iter=30, x0_phys=None, n_per_block=None,
+              max_chunk=None, lam0=1e-2, callback=None, spread=None, block_jacobian="full", stop_lam=None,
+              active_bounds=False, keep_jacobian=False, _internals=False):
+    """Fit every sample at once: shared, per-block and partly free values (joint.py:165-453)."""
+    z = np.atleast_2d(np.asarray(z_meas, np.float64))
+    n, n_pts = z.shape
+    params = experiment.params
+    if n_samples(params) is None:
+        params = tile_params(params, n)
+    if n_samples(params) != n:
+        raise ValueError(f"params carry {n_samples(params)} samples, z_meas {n}")
+    params = SimParams(*[np.asarray(v) for v in params])
+    m0 = np.asarray(experiment.m0, np.float64)
+    if m0.ndim == 1:
+        m0 = np.broadcast_to(m0, (n,) + m0.shape).copy()
+    events, mz = experiment.events, experiment.mz_loc
+    unknown = [s.name for s in spec.slots if s.field not in PSEUDO and s.field not in SimParams._fields]
+    if unknown:
+        raise ValueError(f"{unknown}: not a SimParams field nor one of {PSEUDO}")
+    l_sp = [l for l, s in enumerate(spec.slots) if s.field == "b0_spread"]
+    if l_sp and spread is None:
+        raise ValueError(f"{[spec.slots[l].name for l in l_sp]}: b0_spread needs fit_joint(..., spread=B0Spread(...))")
+    if len(l_sp) > 1:
+        raise ValueError(f"{[spec.slots[l].name for l in l_sp]}: one b0_spread slot at most")
+    sig_held = None if spread is None else np.broadcast_to(np.asarray(spread.sigma_hz, np.float64), (n,)).copy()
+    if block_jacobian not in ("full", "split"):
+        raise ValueError(f"block_jacobian {block_jacobian!r}; use 'full' or 'split'")
+    blocked = any(s.scope == "block" for s in spec.slots)
+    if blocked and (not n_per_block or n_pts % n_per_block):
+        raise ValueError(f"a per-block value needs n_per_block dividing the {n_pts} offsets (got {n_per_block})")
+    nb = n_pts // n_per_block if blocked else 1
+    free, pos, n_loc, cols = _layout(spec, n, nb)
+    P = len(cols)
+    L = spec.n
+    scales = spec.scales
+    is_block = np.array([s.scope == "block" for s in spec.slots])
+    carried = _carried(params, m0, spec, sig_held if sig_held is not None else np.zeros(n))
+    X0 = (np.broadcast_to(spec.x0_phys, free.shape) if x0_phys is None else np.asarray(x0_phys, float))
+    if X0.shape != free.shape:
+        raise ValueError(f"x0_phys has shape {X0.shape}, expected {free.shape} (samples, parameters)")
+    X0 = np.where(free, X0, carried)
+
+    model = _JointModel(params, m0, events, mz, spec, free, pos, n_loc, nb, n_per_block, spread,
+                        sig_held if sig_held is not None else np.zeros(n))
+    model.carried_in = carried
+    # joint column -> local entry of every sample
+    col_of = -np.ones((n, n_loc), int)
+    for p, (l, who, b) in enumerate(cols):
+        for i in who:
+            col_of[i, pos[l] + max(b, 0)] = p
+
+    def locs(x):
+        loc = np.zeros((n, n_loc))
+        for p, (l, who, b) in enumerate(cols):
+            loc[who, pos[l] + max(b, 0)] = x[p]
+        return loc
+
+    def resid(x):
+        return (model.evaluate(locs(x), need_jac=False)[0] - z).reshape(-1)
+
+    def jac(x):
+        Zm, Jl = model.evaluate(locs(x))
+        J = np.zeros((n, n_pts, P))
+        for p, (l, who, b) in enumerate(cols):
+            for i in who:
+                J[i, :, p] += Jl[i, :, pos[l] + max(b, 0)]
+        return J.reshape(-1, P)
+
+    x_start = np.asarray([X0[who[0], l] / scales[l] for l, who, _ in cols], np.float64)
+    if _internals:
+        return dict(resid=resid, jac=jac, x0=x_start, cols=cols, locs=locs, model=model)
+
+    coupled = any(s.scope in ("shared", "block") for s in spec.slots)
+    if not coupled and (stop_lam is not None or active_bounds or keep_jacobian):
+        raise ValueError("stop_lam, active_bounds and keep_jacobian apply to a coupled fit (a shared or "
+                         "per-block value); without one every sample has its own damping, as in `fit`")
+    nan_steps = 0
+    if not coupled:
+        rows, modes = _slot_rows(spec, model.nc)
+        lo, hi = spec.lo_phys / scales, spec.hi_phys / scales
+        hold = None if free.all() else free.astype(np.float64)
+        X0s = X0 / scales
+        chunk = max_chunk or n
+        xs, cs = [], []
+        for a in range(0, n, chunk):
+            b = min(a + chunk, n)
+            sub = SimParams(*[np.asarray(v)[a:b] for v in params])
+            x, c = _lm_device(sub, events, m0[a:b], mz, rows, modes, scales, lo, hi, z[a:b], X0s[a:b], n_iter,
+                              lam0, 0, None if hold is None else hold[a:b], spread,
+                              None if sig_held is None else sig_held[a:b])
+            xs.append(x)
+            cs.append(c)
+        loc = np.concatenate(xs)
+        cost = np.concatenate(cs).sum(axis=0)
+    else:
+        col_slot = np.array([l for l, _, _ in cols], int)
+        col_scale = scales[col_slot]
+        lo = spec.lo_phys[col_slot] / col_scale
+        hi = spec.hi_phys[col_slot] / col_scale
+        shared_cols = [p for p, (l, who, b) in enumerate(cols) if len(who) > 1 or b >= 0]
+        x = x_start.copy()
+        lam, cost = float(lam0), []
+        kept = None
+        for it in range(n_iter):
+            if kept is None:
+                Zm, Jl = model.evaluate(locs(x))
+                r = (Zm - z)
+                finite = bool(np.all(np.isfinite(Jl)))
+            else:
+                (r, Jl), finite = kept, True
+            c = float(np.sum(r * r))
+            if finite:
+                Hl = np.einsum("inj,ink->ijk", Jl, Jl)
+                gl = np.einsum("inj,in->ij", Jl, r)
+                keep = None
+                if active_bounds:
+                    g_full = np.zeros(P)
+                    for i in range(n):
+                        u = np.flatnonzero(col_of[i] >= 0)
+                        np.add.at(g_full, col_of[i][u], gl[i][u])
+                    keep = np.where(((x <= lo) & (g_full > 0)) | ((x >= hi) & (g_full < 0)), 0.0, 1.0)
+                d = _joint_solve(Hl, gl, col_of, shared_cols, P, lam, keep)
+                xn = np.clip(x + d, lo, hi)
+                cn = float(np.sum(resid(xn) ** 2))
+                better = cn < c
+                kept = (r, Jl) if keep_jacobian and not better else None
+                x = xn if better else x
+                lam = lam * 0.5 if better else lam * 3.0
+                cost.append(cn if better else c)
+            else:
+                nan_steps += 1
+                lam = lam * 3.0
+                cost.append(c)
+                kept = None
+            if callback is not None:
+                callback(it, cost[-1])
+            if stop_lam is not None and lam > stop_lam:
+                break
+        loc = locs(x)
+        cost = np.asarray(cost)
+
+    X = np.where(free, loc[:, pos] * scales, carried)
+    Zf, Jl = model.evaluate(loc)
+    r_all = Zf - z
+    sd = np.full(free.shape, np.nan)
+    corr = np.full(free.shape + (L,), np.nan)
+    blocks = {}
+    if not coupled:
+        for i in range(n):
+            use = np.flatnonzero(free[i])
+            if use.size:
+                Ju = Jl[i][:, pos[use]]
+                s2 = float(r_all[i] @ r_all[i]) / max(r_all.shape[1] - use.size, 1)
+                sd[i, use], corr[i][np.ix_(use, use)] = _cov_to_sd_corr(np.linalg.pinv(Ju.T @ Ju) * s2, scales[use])
+    else:
+        J = np.zeros((n, n_pts, P))
+        for p, (l, who, b) in enumerate(cols):
+            for i in who:
+                J[i, :, p] += Jl[i, :, pos[l] + max(b, 0)]
+        J = J.reshape(-1, P)
+        s2 = float(np.sum(r_all ** 2)) / max(r_all.size - P, 1)
+        sd_col, corr_col = _cov_to_sd_corr(np.linalg.pinv(J.T @ J) * s2, col_scale)
+        for i in range(n):
+            ps = [p for p, (l, who, b) in enumerate(cols) if i in who and b < 0]
+            ls = col_slot[ps]
+            sd[i, ls] = sd_col[ps]
+            corr[i][np.ix_(ls, ls)] = corr_col[np.ix_(ps, ps)]
+        for l in np.flatnonzero(is_block):
+            ps = [p for p, (ll, _, b) in enumerate(cols) if ll == l]
+            xb = np.asarray(x, float)[ps] * scales[l]
+            blocks[spec.slots[l].name] = dict(x=xb, sd=sd_col[ps], at_bounds=(
+                np.isclose(xb, spec.slots[l].lo) | np.isclose(xb, spec.slots[l].hi)))
+    X[:, is_block] = np.nan
+    X0 = np.where(is_block[None, :], np.nan, X0)
+    free = free & ~is_block[None, :]
+    return FitResult(X, Zf, z, spec, n_per_block, free=free, sd=sd, corr=corr, x0=X0, cost=cost,
+                     nan_steps=nan_steps, blocks=blocks or None)

@@ -1,0 +1,498 @@
+// bmc_capi.cu -- the C ABI declared in include/bmc_b200.h.
+//
+// Host side of the library: argument checks, a per-device workspace cache, the truncated-Taylor
+// tables, event preprocessing, the dispatch over pool count / precision / tangents per launch,
+// and the device-side Levenberg-Marquardt loop (every launch asynchronous on the caller's stream,
+// no host synchronisation inside a call).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/bmc_b200.h"
+#include "bmc_lm.cuh"
+
+using namespace bmc;
+
+namespace {
+
+thread_local std::string g_err;
+
+bmc_status fail(bmc_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return s;
+}
+
+#define CUDA_TRY(expr)                                                                          \
+    do {                                                                                        \
+        cudaError_t e_ = (expr);                                                                \
+        if (e_ != cudaSuccess) return fail(BMC_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(e_)); \
+    } while (0)
+
+// ------------------------------------------------------------------------------------------------
+// truncated-Taylor tables: theta[m] = max t with t^(m+1)/(m+1)! e^t <= tol (forward bound on the
+// tail of exp, per sub-step), found by bisection
+// ------------------------------------------------------------------------------------------------
+TaylorTable make_table(double tol, int m_max, double dense_theta, double dense_switch) {
+    TaylorTable t{};
+    t.m_max = m_max;
+    t.theta[0] = 0.0;
+    for (int m = 1; m <= kTaylorMMax; ++m) {
+        double lo = 0.0, hi = 64.0;
+        for (int it = 0; it < 200; ++it) {
+            const double mid = 0.5 * (lo + hi);
+            const double lb = (m + 1) * std::log(mid) - std::lgamma(m + 2.0) + mid;
+            if (lb <= std::log(tol)) lo = mid; else hi = mid;
+        }
+        t.theta[m] = lo;
+    }
+    t.dense_theta = dense_theta;
+    int md = 1;
+    while (md < kTaylorMMax && t.theta[md] < dense_theta) ++md;
+    t.dense_m = md;
+    t.dense_switch = dense_switch;
+    return t;
+}
+
+__device__ TaylorTable g_tables[2];   // [BMC_F64, BMC_F32], per device
+
+struct DeviceState {
+    bool tables_ready = false;
+    void* ws = nullptr;
+    size_t ws_bytes = 0;
+};
+std::mutex g_mu;
+std::vector<DeviceState> g_dev;
+
+DeviceState& dev_state(int dev) {
+    if ((int)g_dev.size() <= dev) g_dev.resize(dev + 1);
+    return g_dev[dev];
+}
+
+bmc_status tables(int precision, const TaylorTable** out) {
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_mu);
+    DeviceState& ds = dev_state(dev);
+    if (!ds.tables_ready) {
+        TaylorTable h[2] = {make_table(std::ldexp(1.0, -53), 30, 0.5, 100.0),
+                            make_table(std::ldexp(1.0, -24), 16, 0.5, 100.0)};
+        CUDA_TRY(cudaMemcpyToSymbol(g_tables, h, sizeof(h)));
+        ds.tables_ready = true;
+    }
+    TaylorTable* p = nullptr;
+    CUDA_TRY(cudaGetSymbolAddress((void**)&p, g_tables));
+    *out = p + (precision == BMC_F32 ? 1 : 0);
+    return BMC_OK;
+}
+
+// one cached workspace per device, grown on demand (the caller serialises calls that share it)
+bmc_status workspace(size_t bytes, void** out) {
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_mu);
+    DeviceState& ds = dev_state(dev);
+    if (ds.ws_bytes < bytes) {
+        if (ds.ws) {
+            CUDA_TRY(cudaDeviceSynchronize());
+            CUDA_TRY(cudaFree(ds.ws));
+            ds.ws = nullptr;
+            ds.ws_bytes = 0;
+        }
+        const size_t want = bytes + bytes / 4 + (1 << 20);
+        CUDA_TRY(cudaMalloc(&ds.ws, want));
+        ds.ws_bytes = want;
+    }
+    *out = ds.ws;
+    return BMC_OK;
+}
+
+struct Carve {
+    char* p;
+    size_t used = 0;
+    explicit Carve(void* base) : p((char*)base) {}
+    template <typename T>
+    T* take(size_t n) {
+        used = (used + 255) & ~size_t(255);
+        T* r = (T*)(p + used);
+        used += n * sizeof(T);
+        return r;
+    }
+};
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+bmc_status check_problem(const bmc_problem* pr, const double* params, const bmc_events* ev, const double* m0) {
+    if (!pr || !params || !ev || !m0) return fail(BMC_ERR_INVALID, "null problem, params, events or m0");
+    if (pr->n_voxels < 1 || pr->n_offsets < 1 || pr->n_events < 0)
+        return fail(BMC_ERR_INVALID, "sizes must be positive (voxels %d, offsets %d, events %d)", pr->n_voxels,
+                    pr->n_offsets, pr->n_events);
+    if (pr->n_cest < 0 || pr->n_cest > BMC_MAX_CEST)
+        return fail(BMC_ERR_UNSUPPORTED, "n_cest %d outside 0..%d", pr->n_cest, BMC_MAX_CEST);
+    const int N = 3 * (1 + pr->n_cest) + 1;
+    if (pr->mz_loc >= N) return fail(BMC_ERR_INVALID, "mz_loc %d outside the state (size %d)", pr->mz_loc, N);
+    if (pr->precision != BMC_F64 && pr->precision != BMC_F32)
+        return fail(BMC_ERR_INVALID, "precision %d is neither BMC_F64 nor BMC_F32", pr->precision);
+    if (pr->n_events > 0 && (!ev->d_type || !ev->d_dt || !ev->d_rf_amp || !ev->d_rf_phase || !ev->d_rf_freq))
+        return fail(BMC_ERR_INVALID, "null event field");
+    if (pr->n_offsets > 65535 && pr->n_voxels > 65535)
+        return fail(BMC_ERR_INVALID, "offsets and voxels both above 65535");
+    return BMC_OK;
+}
+
+bool voxel_lanes(const bmc_problem* pr) { return pr->n_voxels >= 64 || pr->n_voxels >= pr->n_offsets; }
+
+bmc_status fill_spread(ChainArgs& a, const bmc_spread* sp) {
+    a.n_nodes = 1;
+    a.sigma = nullptr;
+    a.u[0] = 0.0;
+    a.w[0] = 1.0;
+    if (!sp) return BMC_OK;
+    if (sp->n_nodes < 1 || sp->n_nodes > kMaxNodes || !sp->h_u || !sp->h_w || !sp->d_sigma_hz)
+        return fail(BMC_ERR_INVALID, "spread: 1..%d nodes with u, w and sigma required", kMaxNodes);
+    a.n_nodes = sp->n_nodes;
+    for (int j = 0; j < sp->n_nodes; ++j) {
+        a.u[j] = sp->h_u[j];
+        a.w[j] = sp->h_w[j];
+    }
+    a.sigma = sp->d_sigma_hz;
+    return BMC_OK;
+}
+
+template <typename R>
+bmc_status prep_events(const bmc_problem* pr, const bmc_events* ev, EvRec<R>* out, cudaStream_t st) {
+    const size_t n = (size_t)pr->n_offsets * pr->n_events;
+    if (n == 0) return BMC_OK;
+    const int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+    prep_events_kernel<R><<<blocks, 256, 0, st>>>(pr->n_offsets, pr->n_events, ev->d_type, ev->d_dt, ev->d_rf_amp,
+                                                  ev->d_rf_phase, ev->d_rf_freq, out);
+    CUDA_TRY(cudaGetLastError());
+    return BMC_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// launches
+// ------------------------------------------------------------------------------------------------
+template <int NC, typename R, int NT>
+bmc_status launch_chain(const ChainArgs& a, const TaylorTable* tt, cudaStream_t st) {
+    constexpr int kWarps = 4;
+    const size_t smem = kWarps * sizeof(DenseSmem<NC, R, NT>);
+    CUDA_TRY(cudaFuncSetAttribute(chain_kernel<NC, R, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid = a.voxel_lanes ? dim3((a.n_vox + 127) / 128, a.n_off) : dim3((a.n_off + 127) / 128, a.n_vox);
+    chain_kernel<NC, R, NT><<<grid, kWarps * 32, smem, st>>>(a, tt);
+    CUDA_TRY(cudaGetLastError());
+    return BMC_OK;
+}
+
+// tangents per launch, by pool count (register budget of the dual-number state)
+template <int NC>
+constexpr int tangents_per_pass() { return NC <= 1 ? 2 : 1; }
+
+template <int NC>
+bmc_status run_tangents(ChainArgs a, int P, const TaylorTable* tt, cudaStream_t st) {
+    constexpr int TP = tangents_per_pass<NC>();
+    for (int t0 = 0; t0 < P; t0 += TP) {
+        a.t0 = t0;
+        bmc_status s = (P - t0 >= 2 && TP >= 2) ? launch_chain<NC, double, (TP >= 2 ? 2 : 1)>(a, tt, st)
+                                                : launch_chain<NC, double, 1>(a, tt, st);
+        if (s != BMC_OK) return s;
+    }
+    return BMC_OK;
+}
+
+template <int NC>
+struct Impl {
+    static constexpr int N = Layout<NC>::N;
+
+    static bmc_status simulate(const bmc_problem* pr, const double* params, const bmc_events* ev, const double* m0,
+                               const bmc_spread* sp, double* out, cudaStream_t st) {
+        const TaylorTable* tt = nullptr;
+        bmc_status s = tables(pr->precision, &tt);
+        if (s != BMC_OK) return s;
+        const size_t nrec = (size_t)pr->n_offsets * pr->n_events;
+        void* ws = nullptr;
+        const size_t recb = pr->precision == BMC_F32 ? sizeof(EvRec<float>) : sizeof(EvRec<double>);
+        if ((s = workspace(align256(nrec * recb) + 256, &ws)) != BMC_OK) return s;
+        Carve cv(ws);
+        ChainArgs a{};
+        a.n_vox = pr->n_voxels; a.n_off = pr->n_offsets; a.n_ev = pr->n_events; a.n_fields = Layout<NC>::NF;
+        a.mz = pr->mz_loc; a.reset_after_adc = pr->reset_after_adc; a.voxel_lanes = voxel_lanes(pr) ? 1 : 0;
+        if ((s = fill_spread(a, sp)) != BMC_OK) return s;
+        a.params = params; a.m0 = m0; a.out = out;
+        a.status = cv.take<int>(1);
+        CUDA_TRY(cudaMemsetAsync(a.status, 0, sizeof(int), st));
+        if (pr->precision == BMC_F32) {
+            EvRec<float>* rec = cv.take<EvRec<float>>(nrec);
+            if ((s = prep_events<float>(pr, ev, rec, st)) != BMC_OK) return s;
+            a.ev = rec;
+            return launch_chain<NC, float, 0>(a, tt, st);
+        }
+        EvRec<double>* rec = cv.take<EvRec<double>>(nrec);
+        if ((s = prep_events<double>(pr, ev, rec, st)) != BMC_OK) return s;
+        a.ev = rec;
+        return launch_chain<NC, double, 0>(a, tt, st);
+    }
+
+    static bmc_status trajectory(const bmc_problem* pr, const double* params, const bmc_events* ev,
+                                 const double* m0, double* traj, cudaStream_t st) {
+        const TaylorTable* tt = nullptr;
+        bmc_status s = tables(BMC_F64, &tt);
+        if (s != BMC_OK) return s;
+        const size_t nrec = (size_t)pr->n_offsets * pr->n_events;
+        void* ws = nullptr;
+        if ((s = workspace(align256(nrec * sizeof(EvRec<double>)) + 256 + align256(sizeof(double) * pr->n_voxels * pr->n_offsets), &ws)) != BMC_OK) return s;
+        Carve cv(ws);
+        ChainArgs a{};
+        a.n_vox = pr->n_voxels; a.n_off = pr->n_offsets; a.n_ev = pr->n_events; a.n_fields = Layout<NC>::NF;
+        a.mz = Layout<NC>::izw; a.reset_after_adc = pr->reset_after_adc; a.voxel_lanes = voxel_lanes(pr) ? 1 : 0;
+        fill_spread(a, nullptr);
+        a.params = params; a.m0 = m0; a.traj = traj;
+        a.status = cv.take<int>(1);
+        a.out = cv.take<double>((size_t)pr->n_voxels * pr->n_offsets);
+        CUDA_TRY(cudaMemsetAsync(a.status, 0, sizeof(int), st));
+        EvRec<double>* rec = cv.take<EvRec<double>>(nrec);
+        if ((s = prep_events<double>(pr, ev, rec, st)) != BMC_OK) return s;
+        a.ev = rec;
+        return launch_chain<NC, double, 0>(a, tt, st);
+    }
+
+    static bmc_status jvp(const bmc_problem* pr, const double* params, const bmc_events* ev, const double* m0,
+                          const bmc_spread* sp, const bmc_tangents* tg, double* z, double* jz, cudaStream_t st) {
+        const TaylorTable* tt = nullptr;
+        bmc_status s = tables(BMC_F64, &tt);
+        if (s != BMC_OK) return s;
+        const size_t nrec = (size_t)pr->n_offsets * pr->n_events;
+        void* ws = nullptr;
+        if ((s = workspace(align256(nrec * sizeof(EvRec<double>)) + 256, &ws)) != BMC_OK) return s;
+        Carve cv(ws);
+        ChainArgs a{};
+        a.n_vox = pr->n_voxels; a.n_off = pr->n_offsets; a.n_ev = pr->n_events; a.n_fields = Layout<NC>::NF;
+        a.mz = pr->mz_loc; a.reset_after_adc = pr->reset_after_adc; a.voxel_lanes = voxel_lanes(pr) ? 1 : 0;
+        if ((s = fill_spread(a, sp)) != BMC_OK) return s;
+        a.params = params; a.m0 = m0; a.out = z; a.jout = jz;
+        for (int t = 0; t < tg->n_tangents; ++t) a.field_row[t] = tg->field_row[t];
+        a.seed = tg->d_seed; a.dm0 = tg->d_dm0;
+        a.status = cv.take<int>(1);
+        CUDA_TRY(cudaMemsetAsync(a.status, 0, sizeof(int), st));
+        EvRec<double>* rec = cv.take<EvRec<double>>(nrec);
+        if ((s = prep_events<double>(pr, ev, rec, st)) != BMC_OK) return s;
+        a.ev = rec;
+        return run_tangents<NC>(a, tg->n_tangents, tt, st);
+    }
+
+    static bmc_status lm(const bmc_problem* pr, const double* params, const bmc_events* ev, const double* m0,
+                         const bmc_spread* sp, const bmc_fit_spec* fs, const double* zm, const double* x0,
+                         double* x_out, double* cost_traj, double* x_traj, cudaStream_t st) {
+        const TaylorTable* tt = nullptr;
+        bmc_status s = tables(BMC_F64, &tt);
+        if (s != BMC_OK) return s;
+        const int nv = pr->n_voxels, no = pr->n_offsets, P = fs->n_params;
+        constexpr int NF = Layout<NC>::NF;
+        const size_t nrec = (size_t)no * pr->n_events;
+        const size_t bytes = align256(nrec * sizeof(EvRec<double>)) + 2 * align256(sizeof(double) * NF * nv) +
+                             2 * align256(sizeof(double) * N * nv) + 2 * align256(sizeof(double) * nv) +
+                             align256(sizeof(double) * P * nv) + align256(sizeof(double) * P * nv * N) +
+                             2 * align256(sizeof(double) * nv * no) + align256(sizeof(double) * P * nv * no) +
+                             2 * align256(sizeof(double) * nv * P) + 2 * align256(sizeof(double) * nv) +
+                             align256(sizeof(int) * nv) + 4096;
+        void* ws = nullptr;
+        if ((s = workspace(bytes, &ws)) != BMC_OK) return s;
+        Carve cv(ws);
+        EvRec<double>* rec = cv.take<EvRec<double>>(nrec);
+        double* px = cv.take<double>((size_t)NF * nv);
+        double* pt = cv.take<double>((size_t)NF * nv);
+        double* m0x = cv.take<double>((size_t)N * nv);
+        double* m0t = cv.take<double>((size_t)N * nv);
+        double* sgx = cv.take<double>(nv);
+        double* sgt = cv.take<double>(nv);
+        double* seed = cv.take<double>((size_t)P * nv);
+        double* dm0 = cv.take<double>((size_t)P * nv * N);
+        double* z = cv.take<double>((size_t)nv * no);
+        double* zt = cv.take<double>((size_t)nv * no);
+        double* J = cv.take<double>((size_t)P * nv * no);
+        double* x = cv.take<double>((size_t)nv * P);
+        double* xt = cv.take<double>((size_t)nv * P);
+        double* lam = cv.take<double>(nv);
+        double* cost = cv.take<double>(nv);
+        int* need = cv.take<int>(nv);
+        int* status = cv.take<int>(1);
+        if ((s = prep_events<double>(pr, ev, rec, st)) != BMC_OK) return s;
+        CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), st));
+        CUDA_TRY(cudaMemcpyAsync(x, x0, sizeof(double) * nv * P, cudaMemcpyDeviceToDevice, st));
+        std::vector<double> hl(nv, fs->lam0);
+        std::vector<int> hn(nv, 1);
+        CUDA_TRY(cudaMemcpyAsync(lam, hl.data(), sizeof(double) * nv, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(need, hn.data(), sizeof(int) * nv, cudaMemcpyHostToDevice, st));
+
+        SlotSpec ss{};
+        ss.P = P;
+        bool has_m = false;
+        for (int p = 0; p < P; ++p) {
+            ss.field_row[p] = fs->field_row[p]; ss.mode[p] = fs->mode[p]; ss.scale[p] = fs->scale[p];
+            ss.lo[p] = fs->lo[p]; ss.hi[p] = fs->hi[p];
+            has_m = has_m || fs->field_row[p] == BMC_SLOT_M_START;
+        }
+        ChainArgs a{};
+        a.n_vox = nv; a.n_off = no; a.n_ev = pr->n_events; a.n_fields = NF;
+        a.mz = pr->mz_loc; a.reset_after_adc = pr->reset_after_adc; a.voxel_lanes = voxel_lanes(pr) ? 1 : 0;
+        if ((s = fill_spread(a, sp)) != BMC_OK) return s;
+        const double* sig0 = sp ? sp->d_sigma_hz : nullptr;
+        a.ev = rec; a.status = status;
+        for (int p = 0; p < P; ++p) a.field_row[p] = fs->field_row[p] == BMC_SLOT_M_START ? BMC_SEED_NONE : fs->field_row[p];
+        const int vb = (nv + 127) / 128, wb = (nv + 3) / 4;
+        for (int it = 0; it < fs->n_iter; ++it) {
+            // residual and Jacobian at x, for the voxels whose x moved
+            lm_params_kernel<NC><<<vb, 128, 0, st>>>(nv, ss, params, m0, sig0, x, fs->d_free, px, m0x,
+                                                      sp ? sgx : nullptr, seed, has_m ? dm0 : nullptr);
+            CUDA_TRY(cudaGetLastError());
+            ChainArgs aj = a;
+            aj.params = px; aj.m0 = m0x; aj.sigma = sp ? sgx : nullptr; aj.seed = seed; aj.dm0 = has_m ? dm0 : nullptr;
+            aj.active = need; aj.out = z; aj.jout = J;
+            if ((s = run_tangents<NC>(aj, P, tt, st)) != BMC_OK) return s;
+            lm_solve_kernel<<<wb, 128, 0, st>>>(nv, no, fs->n_points_skip, ss, z, zm, J, fs->d_free, x, lam, cost, xt);
+            CUDA_TRY(cudaGetLastError());
+            // the trial point
+            lm_params_kernel<NC><<<vb, 128, 0, st>>>(nv, ss, params, m0, sig0, xt, fs->d_free, pt, m0t,
+                                                      sp ? sgt : nullptr, nullptr, nullptr);
+            CUDA_TRY(cudaGetLastError());
+            ChainArgs at = a;
+            at.params = pt; at.m0 = m0t; at.sigma = sp ? sgt : nullptr; at.out = zt;
+            if ((s = launch_chain<NC, double, 0>(at, tt, st)) != BMC_OK) return s;
+            lm_accept_kernel<<<wb, 128, 0, st>>>(nv, no, fs->n_points_skip, P, it, fs->n_iter, zt, zm, cost, xt, x,
+                                                 lam, need, cost_traj, x_traj);
+            CUDA_TRY(cudaGetLastError());
+        }
+        CUDA_TRY(cudaMemcpyAsync(x_out, x, sizeof(double) * nv * P, cudaMemcpyDeviceToDevice, st));
+        return BMC_OK;
+    }
+};
+
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------------
+// exported entry points
+// ------------------------------------------------------------------------------------------------
+#define BMC_DISPATCH(nc, call)                                   \
+    switch (nc) {                                                \
+        case 0: return Impl<0>::call;                            \
+        case 1: return Impl<1>::call;                            \
+        case 2: return Impl<2>::call;                            \
+        case 3: return Impl<3>::call;                            \
+        case 4: return Impl<4>::call;                            \
+        case 5: return Impl<5>::call;                            \
+        default: return fail(BMC_ERR_UNSUPPORTED, "n_cest %d", nc); \
+    }
+
+extern "C" {
+
+int32_t bmc_abi_version(void) { return BMC_ABI_VERSION; }
+
+const char* bmc_version(void) { return "bmc_b200 0.1.0 (sm_100a)"; }
+
+size_t bmc_last_error(char* buf, size_t n) {
+    if (buf && n) {
+        const size_t k = std::min(n - 1, g_err.size());
+        std::memcpy(buf, g_err.data(), k);
+        buf[k] = 0;
+    }
+    return g_err.size();
+}
+
+bmc_status bmc_release(void) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    for (size_t d = 0; d < g_dev.size(); ++d) {
+        if (g_dev[d].ws) {
+            cudaSetDevice((int)d);
+            cudaDeviceSynchronize();
+            cudaFree(g_dev[d].ws);
+            g_dev[d].ws = nullptr;
+            g_dev[d].ws_bytes = 0;
+        }
+    }
+    cudaSetDevice(cur);
+    return BMC_OK;
+}
+
+bmc_status bmc_simulate(const bmc_problem* prob, const double* d_params, const bmc_events* ev, const double* d_m0,
+                        const bmc_spread* spread, double* d_out, void* stream) {
+    bmc_status s = check_problem(prob, d_params, ev, d_m0);
+    if (s != BMC_OK) return s;
+    if (!d_out) return fail(BMC_ERR_INVALID, "null output");
+    BMC_DISPATCH(prob->n_cest, simulate(prob, d_params, ev, d_m0, spread, d_out, (cudaStream_t)stream));
+}
+
+bmc_status bmc_simulate_trajectory(const bmc_problem* prob, const double* d_params, const bmc_events* ev,
+                                   const double* d_m0, double* d_traj, void* stream) {
+    bmc_status s = check_problem(prob, d_params, ev, d_m0);
+    if (s != BMC_OK) return s;
+    if (!d_traj) return fail(BMC_ERR_INVALID, "null output");
+    BMC_DISPATCH(prob->n_cest, trajectory(prob, d_params, ev, d_m0, d_traj, (cudaStream_t)stream));
+}
+
+bmc_status bmc_simulate_jvp(const bmc_problem* prob, const double* d_params, const bmc_events* ev,
+                            const double* d_m0, const bmc_spread* spread, const bmc_tangents* tan, double* d_z,
+                            double* d_jz, void* stream) {
+    bmc_status s = check_problem(prob, d_params, ev, d_m0);
+    if (s != BMC_OK) return s;
+    if (!tan || tan->n_tangents < 1 || tan->n_tangents > BMC_MAX_TANGENTS)
+        return fail(BMC_ERR_INVALID, "tangents: 1..%d required", BMC_MAX_TANGENTS);
+    if (!tan->d_seed) return fail(BMC_ERR_INVALID, "tangents: null seed array");
+    if (prob->mz_loc < 0) return fail(BMC_ERR_INVALID, "bmc_simulate_jvp needs mz_loc >= 0");
+    if (prob->precision != BMC_F64) return fail(BMC_ERR_UNSUPPORTED, "tangents are computed in float64 only");
+    if (!d_z || !d_jz) return fail(BMC_ERR_INVALID, "null output");
+    const int nf = BMC_N_FIELDS(prob->n_cest);
+    for (int t = 0; t < tan->n_tangents; ++t)
+        if (tan->field_row[t] >= nf || tan->field_row[t] < BMC_SEED_SPREAD_SIGMA)
+            return fail(BMC_ERR_INVALID, "tangent %d: field row %d outside -2..%d", t, tan->field_row[t], nf - 1);
+    BMC_DISPATCH(prob->n_cest, jvp(prob, d_params, ev, d_m0, spread, tan, d_z, d_jz, (cudaStream_t)stream));
+}
+
+bmc_status bmc_lm_fit(const bmc_problem* prob, const double* d_params, const bmc_events* ev, const double* d_m0,
+                      const bmc_spread* spread, const bmc_fit_spec* spec, const double* d_z_meas, const double* d_x0,
+                      double* d_x_out, double* d_cost_traj, double* d_x_traj, void* stream) {
+    bmc_status s = check_problem(prob, d_params, ev, d_m0);
+    if (s != BMC_OK) return s;
+    if (!spec || spec->n_params < 1 || spec->n_params > BMC_MAX_TANGENTS)
+        return fail(BMC_ERR_INVALID, "fit spec: 1..%d parameters required", BMC_MAX_TANGENTS);
+    if (spec->n_iter < 0) return fail(BMC_ERR_INVALID, "n_iter %d", spec->n_iter);
+    if (prob->mz_loc < 0) return fail(BMC_ERR_INVALID, "bmc_lm_fit needs mz_loc >= 0");
+    if (spec->n_points_skip < 0 || spec->n_points_skip >= prob->n_offsets)
+        return fail(BMC_ERR_INVALID, "n_points_skip %d", spec->n_points_skip);
+    if (!d_z_meas || !d_x0 || !d_x_out) return fail(BMC_ERR_INVALID, "null z_meas, x0 or x_out");
+    const int nf = BMC_N_FIELDS(prob->n_cest);
+    for (int p = 0; p < spec->n_params; ++p) {
+        const int fr = spec->field_row[p];
+        if (fr >= nf || fr < BMC_SLOT_M_START)
+            return fail(BMC_ERR_INVALID, "slot %d: field row %d outside -3..%d", p, fr, nf - 1);
+        if (spec->mode[p] < 0 || spec->mode[p] > 2) return fail(BMC_ERR_INVALID, "slot %d: mode %d", p, spec->mode[p]);
+        if (fr == BMC_SLOT_SPREAD_SIGMA && !spread)
+            return fail(BMC_ERR_INVALID, "slot %d: the spread width needs a spread", p);
+    }
+    BMC_DISPATCH(prob->n_cest, lm(prob, d_params, ev, d_m0, spread, spec, d_z_meas, d_x0, d_x_out, d_cost_traj,
+                                  d_x_traj, (cudaStream_t)stream));
+}
+
+bmc_status bmc_normal_blocks(int32_t n_voxels, int32_t n_points, int32_t n_tangents, const double* d_r,
+                             const double* d_jz, double* d_H, double* d_g, double* d_c, void* stream) {
+    if (n_voxels < 1 || n_points < 1 || n_tangents < 1 || n_tangents > BMC_MAX_TANGENTS)
+        return fail(BMC_ERR_INVALID, "normal blocks: bad sizes (%d, %d, %d)", n_voxels, n_points, n_tangents);
+    if (!d_r || !d_jz || !d_H || !d_g || !d_c) return fail(BMC_ERR_INVALID, "normal blocks: null pointer");
+    normal_blocks_kernel<<<(n_voxels + 3) / 4, 128, 0, (cudaStream_t)stream>>>(n_voxels, n_points, n_tangents, d_r,
+                                                                               d_jz, d_H, d_g, d_c);
+    CUDA_TRY(cudaGetLastError());
+    return BMC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,294 @@
+// bmc_chain.cuh -- the chain kernel: one thread per (voxel, offset), the whole event table.
+//
+// Semantics follow BMC-JAX simulation/simulate.py:22-132 exactly:
+//   * an event evolves the state only if dt > 1e-9 (simulate.py:51);
+//   * GRADIENT and SPOILER zero the x and y entries of water and every CEST pool (simulate.py:55-72);
+//   * last_M is the state after every event; after an ADC the running state returns to M0
+//     (simulate.py:105-114); the result is last_M after the final event (simulate.py:128-132).
+// The time step is exp([A C; 0 0] h)^s [M; 1]; see bmc_device.cuh for how it is evaluated.
+#pragma once
+#include "bmc_device.cuh"
+
+namespace bmc {
+
+constexpr int kMaxNodes = 64;
+constexpr int kMaxT = 8;
+constexpr int kTaylorMMax = 40;
+
+// Truncated-Taylor tables, filled by the host (bmc_capi.cu) for the precision in use:
+// theta[m] = the largest ||X|| for which the degree-m tail bound stays under the tolerance.
+struct TaylorTable {
+    double theta[kTaylorMMax + 1];
+    int m_max;             // short path: degree cap
+    double dense_theta;    // dense path: ||X / 2^s|| <= dense_theta ...
+    int dense_m;           // ... with this Horner degree
+    double dense_switch;   // warps whose largest ||X|| exceeds this take the dense path
+};
+
+struct ChainArgs {
+    int n_vox, n_off, n_ev, n_fields;
+    int mz;                    // state index written; < 0: whole state
+    int reset_after_adc;
+    int voxel_lanes;           // 1: lanes = voxels (events warp-uniform); 0: lanes = offsets
+    int n_nodes;               // spread isochromats (1 = none)
+    double u[kMaxNodes], w[kMaxNodes];
+    const double* params;      // [n_fields][n_vox]
+    const void* ev;            // EvRec<R>[n_ev][n_off]
+    const double* m0;          // [n_vox][N]
+    const double* sigma;       // [n_vox] spread width [Hz] or null
+    // tangents handled by this launch: global tangent indices t0 .. t0 + NT - 1
+    int t0;
+    int field_row[kMaxT];
+    const double* seed;        // [P][n_vox]
+    const double* dm0;         // [P][n_vox][N] or null
+    const int* active;         // [n_vox] or null: voxels with 0 are skipped
+    double* out;               // [n_vox][n_off] (mz >= 0) or [n_vox][n_off][N]
+    double* jout;              // [P][n_vox][n_off] or null
+    double* traj;              // [n_vox][n_off][n_ev][N] or null: the state after every event
+    int* status;               // error flags (bit 0: non-finite norm)
+};
+
+template <int NC>
+struct Layout {
+    static constexpr int N = 3 * NC + 4;        // state size, reference layout
+    static constexpr int NA = N + 1;            // augmented
+    static constexpr int NF = 13 + 5 * NC;      // params rows
+    // params rows (SimParams order, CEST fields expanded)
+    static constexpr int WR1 = 0, WR2 = 1, WF = 2, CK = 3, CF = 3 + NC, CDW = 3 + 2 * NC, CR1 = 3 + 3 * NC,
+                         CR2 = 3 + 4 * NC, MK = 3 + 5 * NC, MF = MK + 1, MDW = MK + 2, MR1 = MK + 3, MR2 = MK + 4,
+                         MLS = MK + 5, B0 = MK + 6, GAM = MK + 7, B0I = MK + 8, RB1 = MK + 9;
+    // reference state indices
+    static constexpr int ixw = 0, iyw = NC + 1, izw = 2 * (NC + 1), izm = 3 * (NC + 1);
+    static __device__ __forceinline__ int ixc(int i) { return 1 + i; }
+    static __device__ __forceinline__ int iyc(int i) { return NC + 2 + i; }
+    static __device__ __forceinline__ int izc(int i) { return 2 * NC + 3 + i; }
+};
+
+template <int NC, typename R, int NT>
+struct Chain {
+    using D = Dn<R, NT>;
+    using L = Layout<NC>;
+    static constexpr int N = L::N;
+    static constexpr int NA = L::NA;
+
+    // ---------------------------------------------------------------------------------------------
+    // parameters -> per-chain constants (matrix.py:99-173), with tangents seeded per field row
+    // ---------------------------------------------------------------------------------------------
+    static __device__ __forceinline__ D field(const ChainArgs& a, int row, int v) {
+        D r = dconst<R, NT>(R(a.params[(size_t)row * a.n_vox + v]));
+        if constexpr (NT > 0) {
+#pragma unroll
+            for (int t = 0; t < NT; ++t)
+                if (a.field_row[a.t0 + t] == row) r.d[t] = R(a.seed[(size_t)(a.t0 + t) * a.n_vox + v]);
+        }
+        return r;
+    }
+
+    static __device__ void load_const(const ChainArgs& a, int v, int node, ChainConst<NC, D>& cc) {
+        const D r1w = field(a, L::WR1, v), r2w = field(a, L::WR2, v);
+        const D b0 = field(a, L::B0, v), gam = field(a, L::GAM, v);
+        D b0i = field(a, L::B0I, v);
+        const D larmor = R(1e6) * (gam * b0);
+        if (a.n_nodes > 1 || a.sigma) {
+            // isochromat `node`: b0_inhom + sigma u / (gamma b0 / 2 pi)   (spread.py:101-104)
+            D sig = dconst<R, NT>(a.sigma ? R(a.sigma[v]) : R(0));
+            if constexpr (NT > 0) {
+#pragma unroll
+                for (int t = 0; t < NT; ++t)
+                    if (a.field_row[a.t0 + t] == -2) sig.d[t] = R(a.seed[(size_t)(a.t0 + t) * a.n_vox + v]);
+            }
+            const D hzpp = R(1.0 / 6.283185307179586) * (gam * b0);
+            b0i = b0i + (R(a.u[node]) * sig) / hzpp;
+        }
+        cc.dw0 = R(1e-6) * (larmor * b0i);
+        D ksum = dconst<R, NT>(R(0));
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+            const D k = field(a, L::CK + i, v), f = field(a, L::CF + i, v);
+            const D r1 = field(a, L::CR1 + i, v), r2 = field(a, L::CR2 + i, v);
+            const D dw = field(a, L::CDW + i, v);
+            cc.k[i] = k;
+            cc.kwc[i] = k * f;
+            ksum = ksum + cc.kwc[i];
+            cc.Rc2[i] = r2 + k;
+            cc.Rc1[i] = r1 + k;
+            cc.cc[i] = r1 * f;
+            cc.offc0[i] = R(1e-6) * (dw * larmor);
+        }
+        const D kmt = field(a, L::MK, v), fmt = field(a, L::MF, v), r1mt = field(a, L::MR1, v);
+        const D r2mt = field(a, L::MR2, v), dwmt = field(a, L::MDW, v);
+        cc.kmt = kmt;
+        cc.kwmt = kmt * fmt;
+        cc.Rm1 = r1mt + kmt;
+        cc.cm = r1mt * fmt;
+        cc.Rw2 = r2w + ksum;
+        cc.Rw1 = (r1w + ksum) + cc.kwmt;
+        cc.cw = r1w;
+        cc.relb1 = field(a, L::RB1, v);
+        cc.dwmt = R(1e-6) * (dwmt * larmor);
+        cc.t2mt = dconst<R, NT>(R(1)) / r2mt;
+        cc.w0sl = R(1e-6) * larmor;
+        int ls = (int)a.params[(size_t)L::MLS * a.n_vox + v];
+        cc.ls = ls < 0 ? 0 : (ls > 2 ? 2 : ls);
+        cc.mt_on = fmt.v > R(1e-9);
+    }
+
+    // ---------------------------------------------------------------------------------------------
+    // one event's coefficients (unscaled) and the infinity norm of its generator times dt
+    // ---------------------------------------------------------------------------------------------
+    static __device__ __forceinline__ void event_coef(const ChainConst<NC, D>& cc, const EvRec<R>& e, D g_mt,
+                                                      StepCoef<NC, D>& sc) {
+        const D offw = e.wf - cc.dw0;                                  // matrix.py:162
+        const D w1 = e.w1 * cc.relb1;                                  // matrix.py:121
+        sc.offw = offw;
+        sc.w1x = e.c * w1;
+        sc.w1y = e.s * w1;
+        sc.Rw2 = cc.Rw2;
+        sc.Rw1 = cc.Rw1;
+        sc.cw = cc.cw;
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+            sc.k[i] = cc.k[i];
+            sc.kwc[i] = cc.kwc[i];
+            sc.Rc2[i] = cc.Rc2[i];
+            sc.Rc1[i] = cc.Rc1[i];
+            sc.cc[i] = cc.cc[i];
+            sc.offc[i] = cc.offc0[i] - offw;                           // matrix.py:166
+        }
+        sc.kmt = cc.kmt;
+        sc.kwmt = cc.kwmt;
+        sc.Rm1W = cc.Rm1 + (w1 * w1) * g_mt;                           // matrix.py:210, 283
+        sc.cm = cc.cm;
+    }
+
+    static __device__ __forceinline__ R coef_norm(const StepCoef<NC, D>& s) {
+        R sk = R(0);
+#pragma unroll
+        for (int i = 0; i < NC; ++i) sk += fabs(s.k[i].v);
+        const R ax = fabs(s.w1x.v), ay = fabs(s.w1y.v), ow = fabs(s.offw.v);
+        R m = fabs(s.Rw2.v) + ow + fmax(ax, ay) + sk;
+        m = fmax(m, ax + ay + fabs(s.Rw1.v) + sk + fabs(s.kmt.v) + fabs(s.cw.v));
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+            const R b = fabs(s.kwc[i].v);
+            m = fmax(m, fabs(s.Rc2[i].v) + fabs(s.offc[i].v) + fmax(ax, ay) + b);
+            m = fmax(m, ax + ay + fabs(s.Rc1[i].v) + b + fabs(s.cc[i].v));
+        }
+        m = fmax(m, fabs(s.Rm1W.v) + fabs(s.kwmt.v) + fabs(s.cm.v));
+        return m;
+    }
+
+    static __device__ __forceinline__ void scale_coef(StepCoef<NC, D>& s, R h) {
+        s.Rw2 = h * s.Rw2; s.Rw1 = h * s.Rw1; s.cw = h * s.cw;
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+            s.k[i] = h * s.k[i]; s.kwc[i] = h * s.kwc[i]; s.Rc2[i] = h * s.Rc2[i];
+            s.Rc1[i] = h * s.Rc1[i]; s.cc[i] = h * s.cc[i]; s.offc[i] = h * s.offc[i];
+        }
+        s.offw = h * s.offw; s.w1x = h * s.w1x; s.w1y = h * s.w1y;
+        s.kmt = h * s.kmt; s.kwmt = h * s.kwmt; s.Rm1W = h * s.Rm1W; s.cm = h * s.cm;
+    }
+
+    // y = X v (+ C h when WithC): the sparse Bloch-McConnell operator (matrix.py:238-293)
+    template <bool WithC>
+    static __device__ __forceinline__ void matvec(const StepCoef<NC, D>& s, const State<NC, D>& v, State<NC, D>& y) {
+        D xw = dfma(s.offw, v.yw, -(s.Rw2 * v.xw));
+        xw = xw - s.w1y * v.zw;
+        D yw = dfma(s.w1x, v.zw, -(s.Rw2 * v.yw));
+        yw = yw - s.offw * v.xw;
+        D zw = dfma(s.w1y, v.xw, -(s.Rw1 * v.zw));
+        zw = zw - s.w1x * v.yw;
+        zw = dfma(s.kmt, v.zm, zw);
+        if constexpr (WithC) zw = zw + s.cw;
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+            xw = dfma(s.k[i], v.xc[i], xw);
+            yw = dfma(s.k[i], v.yc[i], yw);
+            zw = dfma(s.k[i], v.zc[i], zw);
+            D xc = dfma(s.kwc[i], v.xw, -(s.Rc2[i] * v.xc[i]));
+            xc = xc - s.offc[i] * v.yc[i];
+            xc = xc - s.w1y * v.zc[i];
+            D yc = dfma(s.kwc[i], v.yw, -(s.Rc2[i] * v.yc[i]));
+            yc = dfma(s.offc[i], v.xc[i], yc);
+            yc = dfma(s.w1x, v.zc[i], yc);
+            D zc = dfma(s.kwc[i], v.zw, -(s.Rc1[i] * v.zc[i]));
+            zc = dfma(s.w1y, v.xc[i], zc);
+            zc = zc - s.w1x * v.yc[i];
+            if constexpr (WithC) zc = zc + s.cc[i];
+            y.xc[i] = xc;
+            y.yc[i] = yc;
+            y.zc[i] = zc;
+        }
+        D zm = dfma(s.kwmt, v.zw, -(s.Rm1W * v.zm));
+        if constexpr (WithC) zm = zm + s.cm;
+        y.xw = xw;
+        y.yw = yw;
+        y.zw = zw;
+        y.zm = zm;
+    }
+
+    static __device__ __forceinline__ void axpy_state(State<NC, D>& acc, const State<NC, D>& t) {
+        acc.xw = acc.xw + t.xw; acc.yw = acc.yw + t.yw; acc.zw = acc.zw + t.zw; acc.zm = acc.zm + t.zm;
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+            acc.xc[i] = acc.xc[i] + t.xc[i]; acc.yc[i] = acc.yc[i] + t.yc[i]; acc.zc[i] = acc.zc[i] + t.zc[i];
+        }
+    }
+    static __device__ __forceinline__ void scal_state(State<NC, D>& t, R a) {
+        t.xw = a * t.xw; t.yw = a * t.yw; t.zw = a * t.zw; t.zm = a * t.zm;
+#pragma unroll
+        for (int i = 0; i < NC; ++i) { t.xc[i] = a * t.xc[i]; t.yc[i] = a * t.yc[i]; t.zc[i] = a * t.zc[i]; }
+    }
+
+    // exp(X)^s [M; 1] by s sub-steps of the degree-m Taylor polynomial; s applies to X already scaled
+    static __device__ __forceinline__ void taylor_apply(const StepCoef<NC, D>& s, int nsub, int m, State<NC, D>& M) {
+        for (int j = 0; j < nsub; ++j) {
+            State<NC, D> term, acc = M;
+            matvec<true>(s, M, term);
+            axpy_state(acc, term);
+            for (int k = 2; k <= m; ++k) {
+                State<NC, D> nt;
+                matvec<false>(s, term, nt);
+                scal_state(nt, R(1) / R(k));
+                term = nt;
+                axpy_state(acc, term);
+            }
+            M = acc;
+        }
+    }
+
+    static __device__ __forceinline__ void spoil(State<NC, D>& M) {
+        const D z = dconst<R, NT>(R(0));
+        M.xw = z; M.yw = z;
+#pragma unroll
+        for (int i = 0; i < NC; ++i) { M.xc[i] = z; M.yc[i] = z; }
+    }
+
+    static __device__ __forceinline__ D& at(State<NC, D>& M, int ref_index) {
+        // reference index -> member (used only outside hot loops)
+        if (ref_index == L::ixw) return M.xw;
+        if (ref_index == L::iyw) return M.yw;
+        if (ref_index == L::izw) return M.zw;
+        if (ref_index == L::izm) return M.zm;
+        if (ref_index <= NC) return M.xc[ref_index - 1];
+        if (ref_index <= 2 * NC + 1) return M.yc[ref_index - NC - 2];
+        return M.zc[ref_index - 2 * NC - 3];
+    }
+
+    static __device__ void load_m0(const ChainArgs& a, int v, State<NC, D>& M) {
+        const double* m0 = a.m0 + (size_t)v * N;
+#pragma unroll
+        for (int q = 0; q < N; ++q) {
+            D x = dconst<R, NT>(R(m0[q]));
+            if constexpr (NT > 0) {
+                if (a.dm0) {
+#pragma unroll
+                    for (int t = 0; t < NT; ++t) x.d[t] = R(a.dm0[((size_t)(a.t0 + t) * a.n_vox + v) * N + q]);
+                }
+            }
+            at(M, q) = x;
+        }
+    }
+};
+
+}  // namespace bmc

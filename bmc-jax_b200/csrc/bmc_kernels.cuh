@@ -1,0 +1,287 @@
+// bmc_kernels.cuh -- the chain kernel, its dense long-event path, and the event preprocessing.
+#pragma once
+#include "bmc_chain.cuh"
+
+namespace bmc {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+template <typename R>
+__device__ __forceinline__ R warp_max(R x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(kFull, x, o));
+    return x;
+}
+
+// ------------------------------------------------------------------------------------------------
+// dense path: a warp exponentiates one chain's generator at a time, lane j owning column j
+// ------------------------------------------------------------------------------------------------
+// For an event whose generator X = [A C; 0 0] dt has a large norm (a long delay or CW block), the
+// Taylor action would need ~||X|| sub-steps. Instead the warp forms exp(X) by scaling and squaring:
+// exp(X / 2^s) by a degree-m Horner recurrence (each column by the sparse operator, in registers),
+// then s squarings through shared memory, then the matrix-vector product with [M; 1].
+template <int NC, typename R, int NT>
+struct DenseSmem {
+    using D = Dn<R, NT>;
+    static constexpr int NA = Layout<NC>::NA;
+    StepCoef<NC, D> coef;           // the owner chain's coefficients, scaled by dt / 2^s
+    D mat[NA * NA];                 // column-major: column j at [j * NA]
+    D vec[NA];                      // the owner's [M; 1]
+    D out[NA];
+    int s;
+};
+
+template <int NC, typename R, int NT>
+struct Dense {
+    using D = Dn<R, NT>;
+    using C = Chain<NC, R, NT>;
+    using L = Layout<NC>;
+    static constexpr int N = L::N;
+    static constexpr int NA = L::NA;
+    using SM = DenseSmem<NC, R, NT>;
+
+    // y = X_A v + C * caug: one column of X times a column of the matrix being built
+    static __device__ __forceinline__ void matvec_aug(const StepCoef<NC, D>& s, const State<NC, D>& v, R caug,
+                                                      State<NC, D>& y) {
+        C::template matvec<false>(s, v, y);
+        if (caug != R(0)) {
+            y.zw = y.zw + caug * s.cw;
+            y.zm = y.zm + caug * s.cm;
+#pragma unroll
+            for (int i = 0; i < NC; ++i) y.zc[i] = y.zc[i] + caug * s.cc[i];
+        }
+    }
+
+    static __device__ __forceinline__ void unit(State<NC, D>& col, int j) {
+        const D z = dconst<R, NT>(R(0));
+        col.xw = z; col.yw = z; col.zw = z; col.zm = z;
+#pragma unroll
+        for (int i = 0; i < NC; ++i) { col.xc[i] = z; col.yc[i] = z; col.zc[i] = z; }
+#pragma unroll
+        for (int q = 0; q < N; ++q)
+            if (q == j) C::at(col, q) = dconst<R, NT>(R(1));
+    }
+
+    static __device__ void event(SM* sm, int lane, bool evolve, const StepCoef<NC, D>& sc, R dt, R nu,
+                                 State<NC, D>& M, const TaylorTable& tt, int* status) {
+        unsigned need = __ballot_sync(kFull, evolve);
+        while (need) {
+            const int c = __ffs(need) - 1;
+            need &= need - 1;
+            if (lane == c) {
+                int s = 0;
+                if (nu > R(tt.dense_theta)) s = (int)ceil(log2(double(nu) / tt.dense_theta));
+                if (s > 200) {
+                    s = 200;
+                    atomicOr(status, 2);
+                }
+                StepCoef<NC, D> scs = sc;
+                C::scale_coef(scs, R(ldexp(double(dt), -s)));
+                sm->coef = scs;
+                sm->s = s;
+#pragma unroll
+                for (int q = 0; q < N; ++q) sm->vec[q] = C::at(M, q);
+                sm->vec[N] = dconst<R, NT>(R(1));
+            }
+            __syncwarp();
+            const int s = sm->s;
+            State<NC, D> col;
+            const R caug = (lane == N) ? R(1) : R(0);
+            // Horner: T = I + X T / k, k = m .. 1  (column `lane`)
+            unit(col, lane);
+            if (lane < NA) {
+                for (int k = tt.dense_m; k >= 1; --k) {
+                    State<NC, D> y;
+                    matvec_aug(sm->coef, col, caug, y);
+                    C::scal_state(y, R(1) / R(k));
+                    State<NC, D> e;
+                    unit(e, lane);
+                    C::axpy_state(e, y);
+                    col = e;
+                }
+            }
+            // s squarings: column j of T T is sum_l T[:, l] T[l][j]
+            for (int q = 0; q < s; ++q) {
+                if (lane < NA) {
+#pragma unroll
+                    for (int i = 0; i < N; ++i) sm->mat[lane * NA + i] = C::at(col, i);
+                    sm->mat[lane * NA + N] = dconst<R, NT>(caug);
+                }
+                __syncwarp();
+                if (lane < NA) {
+                    State<NC, D> nc;
+                    unit(nc, -1);
+#pragma unroll
+                    for (int l = 0; l < N; ++l) {
+                        const D w = C::at(col, l);
+#pragma unroll
+                        for (int i = 0; i < N; ++i) C::at(nc, i) = dfma(sm->mat[l * NA + i], w, C::at(nc, i));
+                    }
+                    if (caug != R(0)) {           // the augmented column also picks up T[:, aug]
+#pragma unroll
+                        for (int i = 0; i < N; ++i) C::at(nc, i) = C::at(nc, i) + sm->mat[N * NA + i];
+                    }
+                    col = nc;
+                }
+                __syncwarp();
+            }
+            // M <- T [M; 1]
+            if (lane < NA) {
+#pragma unroll
+                for (int i = 0; i < N; ++i) sm->mat[lane * NA + i] = C::at(col, i);
+            }
+            __syncwarp();
+            if (lane < N) {
+                D acc = dconst<R, NT>(R(0));
+                for (int j = 0; j < NA; ++j) acc = dfma(sm->mat[j * NA + lane], sm->vec[j], acc);
+                sm->out[lane] = acc;
+            }
+            __syncwarp();
+            if (lane == c) {
+#pragma unroll
+                for (int q = 0; q < N; ++q) C::at(M, q) = sm->out[q];
+            }
+            __syncwarp();
+        }
+    }
+};
+
+// ------------------------------------------------------------------------------------------------
+// the chain kernel
+// ------------------------------------------------------------------------------------------------
+template <int NC, typename R, int NT>
+__global__ void __launch_bounds__(128) chain_kernel(const ChainArgs a, const TaylorTable* __restrict__ ttab) {
+    using D = Dn<R, NT>;
+    using C = Chain<NC, R, NT>;
+    using SM = DenseSmem<NC, R, NT>;
+    constexpr int N = Layout<NC>::N;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    SM* dsm = reinterpret_cast<SM*>(smem_raw) + (threadIdx.x >> 5);
+    const TaylorTable& tt = *ttab;
+
+    const int ia = blockIdx.x * blockDim.x + threadIdx.x;
+    int v, o;
+    bool valid;
+    if (a.voxel_lanes) {
+        v = ia; o = blockIdx.y; valid = v < a.n_vox;
+    } else {
+        o = ia; v = blockIdx.y; valid = o < a.n_off;
+    }
+    if (!valid) {
+        v = v < a.n_vox ? v : a.n_vox - 1;
+        o = o < a.n_off ? o : a.n_off - 1;
+    }
+    const bool act = valid && (a.active == nullptr || a.active[v] != 0);
+    if (__all_sync(kFull, !act)) return;
+    const EvRec<R>* __restrict__ ev = reinterpret_cast<const EvRec<R>*>(a.ev);
+
+    const size_t ch = (size_t)v * a.n_off + o;
+    for (int node = 0; node < a.n_nodes; ++node) {
+        ChainConst<NC, D> cc;
+        C::load_const(a, v, node, cc);
+        State<NC, D> M;
+        C::load_m0(a, v, M);
+        bool reset_pending = false;
+        R gkey = R(NAN);
+        D gval = dconst<R, NT>(R(0));
+        for (int e = 0; e < a.n_ev; ++e) {
+            const EvRec<R> rec = ev[(size_t)e * a.n_off + o];
+            if (reset_pending) {                                   // the ADC reset of the previous event
+                C::load_m0(a, v, M);
+                reset_pending = false;
+            }
+            const int type = (int)rec.type;
+            const bool evolve = act && rec.dt > R(1e-9);
+            if (__any_sync(kFull, evolve)) {
+                D g = dconst<R, NT>(R(0));
+                if (cc.mt_on && cc.ls != 0 && rec.w1 != R(0)) {
+                    if (rec.wf != gkey) {
+                        gkey = rec.wf;
+                        const D offmt = (rec.wf - cc.dw0) - cc.dwmt;
+                        gval = cc.ls == 1 ? lorentzian<R, NT>(offmt, cc.t2mt)
+                                          : super_lorentzian<R, NT>(offmt, cc.t2mt, cc.w0sl);
+                    }
+                    g = gval;
+                }
+                StepCoef<NC, D> sc;
+                C::event_coef(cc, rec, g, sc);
+                R nu = evolve ? rec.dt * C::coef_norm(sc) : R(0);
+                if (!(nu < R(INFINITY))) {                          // NaN or inf: flag, let NaN propagate
+                    if (evolve) atomicOr(a.status, 1);
+                    nu = R(0);
+                }
+                const R numax = warp_max(nu);
+                if (numax > R(tt.dense_switch)) {
+                    Dense<NC, R, NT>::event(dsm, lane, evolve, sc, rec.dt, nu, M, tt, a.status);
+                } else if (numax > R(0)) {
+                    int m = 1, nsub = 1;
+                    const R thm = R(tt.theta[tt.m_max]);
+                    if (numax > thm) nsub = (int)ceil(numax / thm);
+                    const R per = numax / R(nsub);
+                    while (m < tt.m_max && R(tt.theta[m]) < per) ++m;
+                    C::scale_coef(sc, rec.dt / R(nsub));
+                    State<NC, D> Mn = M;
+                    C::taylor_apply(sc, nsub, m, Mn);
+                    if (evolve) M = Mn;
+                }
+            }
+            if (type == EV_GRADIENT || type == EV_SPOILER) C::spoil(M);
+            if (a.traj != nullptr && act) {
+                double* tp = a.traj + (ch * a.n_ev + e) * N;
+#pragma unroll
+                for (int q = 0; q < N; ++q) tp[q] = double(C::at(M, q).v);
+            }
+            if (type == EV_ADC && a.reset_after_adc) reset_pending = (e + 1 < a.n_ev);
+        }
+        // last_M of this isochromat, weighted into the spread mean (written by the chain's own thread)
+        if (act) {
+            const R wgt = a.n_nodes > 1 ? R(a.w[node]) : R(1);
+            if (a.mz >= 0) {
+                D z = dconst<R, NT>(R(0));
+#pragma unroll
+                for (int q = 0; q < N; ++q)
+                    if (q == a.mz) z = C::at(M, q);
+                a.out[ch] = (node ? a.out[ch] : 0.0) + double(wgt * z.v);
+                if constexpr (NT > 0) {
+                    if (a.jout) {
+#pragma unroll
+                        for (int t = 0; t < NT; ++t) {
+                            double* jp = a.jout + ((size_t)(a.t0 + t) * a.n_vox + v) * a.n_off + o;
+                            *jp = (node ? *jp : 0.0) + double(wgt * z.d[t]);
+                        }
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < N; ++q)
+                    a.out[ch * N + q] = (node ? a.out[ch * N + q] : 0.0) + double(wgt * C::at(M, q).v);
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// event preprocessing: the reference table [n_off][n_ev] -> records [n_ev][n_off]
+// ------------------------------------------------------------------------------------------------
+template <typename R>
+__global__ void prep_events_kernel(int n_off, int n_ev, const int32_t* __restrict__ type, const double* __restrict__ dt,
+                                   const double* __restrict__ amp, const double* __restrict__ phase,
+                                   const double* __restrict__ freq, EvRec<R>* __restrict__ out) {
+    const size_t n = (size_t)n_off * n_ev;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t o = i / n_ev, e = i % n_ev;
+        EvRec<R> r;
+        r.dt = R(dt[i]);
+        r.w1 = R(6.283185307179586 * amp[i]);
+        double s, c;
+        sincos(phase[i], &s, &c);
+        r.c = R(c);
+        r.s = R(s);
+        r.wf = R(6.283185307179586 * freq[i]);
+        r.type = R(type[i]);
+        out[e * n_off + o] = r;
+    }
+}
+
+}  // namespace bmc

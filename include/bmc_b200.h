@@ -1,0 +1,180 @@
+/*
+ * bmc_b200.h -- C ABI of the B200 (sm_100a) Bloch-McConnell simulator and Levenberg-Marquardt fitter.
+ *
+ * Plain C: pointers, sizes and status codes; no C++ or torch types cross this boundary.
+ * Every pointer named `d_*` is DEVICE memory owned by the caller; `h_*` is host memory.
+ * Every call is asynchronous on the given CUDA stream (`stream` is a cudaStream_t, NULL = legacy
+ * default stream) and returns a status; `bmc_last_error` gives the message of the last failure
+ * on the calling thread. Exceptions never cross the ABI.
+ *
+ * Data layout (the reference's, BMC-JAX simulation/params.py:18-49 and simulation/events.py:20-32):
+ *   params   d_params[n_fields][n_voxels], float64, rows in SimParams order with every CEST field
+ *            expanded into n_cest rows:
+ *              water_r1, water_r2, water_f, cest_k[n_cest], cest_f[n_cest], cest_dw[n_cest],
+ *              cest_r1[n_cest], cest_r2[n_cest], mt_k, mt_f, mt_dw, mt_r1, mt_r2,
+ *              mt_lineshape (0 none, 1 Lorentzian, 2 super-Lorentzian, as a float), b0, gamma,
+ *              b0_inhom, rel_b1.            n_fields = 13 + 5 n_cest   (BMC_N_FIELDS)
+ *   events   six arrays [n_offsets][n_events] (row-major by offset): type int32 (0 DELAY,
+ *            1 RF_PULSE, 2 GRADIENT, 3 ADC, 4 SPOILER), dt [s], rf_amp [Hz], rf_phase [rad],
+ *            rf_freq [Hz] float64, adc_idx int32 (carried, not used by the solver).
+ *   state    N = 3 (1 + n_cest) + 1 entries: water x, CEST x..., water y, CEST y..., water z,
+ *            CEST z..., MT z (simulation/matrix.py:224-234). d_m0[n_voxels][N].
+ *   output   Z[n_voxels][n_offsets] = state[mz_loc] after the last event of every offset, or
+ *            the whole state [n_voxels][n_offsets][N] when mz_loc < 0.
+ */
+#ifndef BMC_B200_H
+#define BMC_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BMC_ABI_VERSION 1
+#define BMC_MAX_CEST 5             /* water + up to five CEST pools + MT: N <= 19 */
+#define BMC_MAX_TANGENTS 8
+#define BMC_N_FIELDS(n_cest) (13 + 5 * (n_cest))
+
+typedef enum {
+    BMC_OK = 0,
+    BMC_ERR_INVALID = 1,           /* a size, pointer or option is out of range */
+    BMC_ERR_CUDA = 2,              /* a CUDA runtime call failed */
+    BMC_ERR_UNSUPPORTED = 3,       /* e.g. n_cest above BMC_MAX_CEST */
+    BMC_ERR_NUMERIC = 4,           /* a chain needed more squarings than the cap: its outputs are NaN */
+} bmc_status;
+
+/* precision of the propagation arithmetic */
+#define BMC_F64 0
+#define BMC_F32 1
+
+/* special tangent seeds (bmc_tangents.field_row) */
+#define BMC_SEED_NONE (-1)         /* only d_dm0 drives this tangent */
+#define BMC_SEED_SPREAD_SIGMA (-2) /* derivative with respect to the B0-spread width sigma [Hz] */
+
+typedef struct {
+    int32_t n_voxels;
+    int32_t n_offsets;
+    int32_t n_events;
+    int32_t n_cest;                /* 0 .. BMC_MAX_CEST */
+    int32_t mz_loc;                /* state index returned as Z; < 0 returns the full state */
+    int32_t reset_after_adc;       /* 1: the state returns to M0 after every ADC (reference default) */
+    int32_t precision;             /* BMC_F64 or BMC_F32 */
+    int32_t reserved;
+} bmc_problem;
+
+typedef struct {
+    const int32_t* d_type;
+    const double* d_dt;
+    const double* d_rf_amp;
+    const double* d_rf_phase;
+    const double* d_rf_freq;
+    const int32_t* d_adc_idx;      /* may be NULL */
+} bmc_events;
+
+/* B0 spread inside a voxel (simulation/spread.py:38-106): Z is the weighted mean over n_nodes
+ * isochromats, node j at b0_inhom + sigma u_j / (gamma b0 / 2 pi). NULL spread = one isochromat. */
+typedef struct {
+    int32_t n_nodes;               /* <= 64 */
+    const double* h_u;             /* [n_nodes] offsets in units of sigma */
+    const double* h_w;             /* [n_nodes] weights, summing to 1 */
+    const double* d_sigma_hz;      /* [n_voxels] width per voxel [Hz] */
+} bmc_spread;
+
+/* Forward-mode tangents: tangent p seeds d(field_row[p]) = d_seed[p][voxel] (per voxel) and
+ * dM0 = d_dm0[p][voxel][N] (NULL = 0). BMC_SEED_SPREAD_SIGMA seeds d(sigma) instead of a field. */
+typedef struct {
+    int32_t n_tangents;            /* 1 .. BMC_MAX_TANGENTS */
+    int32_t field_row[BMC_MAX_TANGENTS];
+    const double* d_seed;          /* [n_tangents][n_voxels] */
+    const double* d_dm0;           /* [n_tangents][n_voxels][N] or NULL */
+} bmc_tangents;
+
+/* Free parameters of a Levenberg-Marquardt fit (fitting/params.py:38-112, fitting/joint.py:99-138).
+ * Slot p writes x_phys = x_scaled * scale[p] into params row field_row[p] as
+ *   mode 0 "value": field = x_phys;  1 "factor": field = base * x_phys;  2 "add": field = base + x_phys
+ * or, for field_row == BMC_SLOT_M_START, scales the start state (mode 0: initial_state(params) * x,
+ * rebuilt from the current pools; mode 1: d_m0 * x), or for BMC_SLOT_SPREAD_SIGMA sets the spread
+ * width. Where d_free[v][p] == 0 the slot is held at its carried value and its step is exactly zero. */
+#define BMC_SLOT_M_START (-3)
+#define BMC_SLOT_SPREAD_SIGMA (-2)
+typedef struct {
+    int32_t n_params;              /* 1 .. BMC_MAX_TANGENTS */
+    int32_t n_iter;
+    double lam0;
+    int32_t field_row[BMC_MAX_TANGENTS];
+    int32_t mode[BMC_MAX_TANGENTS];
+    double scale[BMC_MAX_TANGENTS];
+    double lo[BMC_MAX_TANGENTS];   /* bounds, scaled units */
+    double hi[BMC_MAX_TANGENTS];
+    const double* d_free;          /* [n_voxels][n_params] 1/0, or NULL = all free */
+    int32_t n_points_skip;         /* leading simulated offsets left out of the residual (skip_first) */
+    int32_t reserved;
+} bmc_fit_spec;
+
+/* Library identity. */
+int32_t bmc_abi_version(void);
+const char* bmc_version(void);
+
+/* Message of the last non-OK status on this thread (copied, NUL-terminated). Returns its length. */
+size_t bmc_last_error(char* buf, size_t buf_len);
+
+/* Free the cached device workspaces of every device (call with no work in flight). */
+bmc_status bmc_release(void);
+
+/*
+ * Forward model. Replaces simulation/simulate.py:134-148 (simulate_spectrum, vmapped over offsets),
+ * simulation/voxels.py:89-129 (simulate_voxels), simulation/spread.py:77-106
+ * (simulate_spectrum_spread, with `spread`) and fitting/experiment.py:58-61 (Experiment.simulate).
+ * d_out: [n_voxels][n_offsets] (mz_loc >= 0) or [n_voxels][n_offsets][N].
+ */
+bmc_status bmc_simulate(const bmc_problem* prob, const double* d_params, const bmc_events* ev,
+                        const double* d_m0, const bmc_spread* spread, double* d_out, void* stream);
+
+/*
+ * Forward model, keeping the state after every event (the reference's return_full_trajectory=True,
+ * simulation/simulate.py:80-132): d_traj[n_voxels][n_offsets][n_events][N], float64 propagation.
+ */
+bmc_status bmc_simulate_trajectory(const bmc_problem* prob, const double* d_params, const bmc_events* ev,
+                                   const double* d_m0, double* d_traj, void* stream);
+
+/*
+ * Forward model and its forward-mode tangents: Z and dZ along each seeded direction.
+ * Replaces the jax.jacfwd of the model in fitting/lm.py:39, fitting/joint.py:300,317 and
+ * design/crlb.py:57. d_z: [n_voxels][n_offsets]; d_jz: [n_tangents][n_voxels][n_offsets]
+ * (state index prob->mz_loc, which must be >= 0).
+ */
+bmc_status bmc_simulate_jvp(const bmc_problem* prob, const double* d_params, const bmc_events* ev,
+                            const double* d_m0, const bmc_spread* spread, const bmc_tangents* tan,
+                            double* d_z, double* d_jz, void* stream);
+
+/*
+ * Bounded Levenberg-Marquardt of every voxel, all iterations on the device.
+ * Replaces fitting/lm.py:20-67 as driven by fitting/independent.py:51-129 (fit_batch, vmapped over
+ * voxels) and the uncoupled branch of fitting/joint.py:359-374 (per-sample damping, `free` holds).
+ * d_z_meas: [n_voxels][n_offsets - n_points_skip]; d_x0: [n_voxels][n_params] scaled units.
+ * d_x_out: [n_voxels][n_params] scaled. d_cost_traj: [n_voxels][n_iter] or NULL (the cost after each
+ * step, fitting/lm.py:61). d_x_traj: [n_voxels][n_iter][n_params] or NULL.
+ * The float64 normal equations are solved by Gaussian elimination with partial pivoting.
+ */
+bmc_status bmc_lm_fit(const bmc_problem* prob, const double* d_params, const bmc_events* ev,
+                      const double* d_m0, const bmc_spread* spread, const bmc_fit_spec* spec,
+                      const double* d_z_meas, const double* d_x0, double* d_x_out,
+                      double* d_cost_traj, double* d_x_traj, void* stream);
+
+/*
+ * Per-sample normal-equation blocks for a coupled joint fit (fitting/joint.py:149-162, 344-348):
+ * for every voxel v, H_v = J_v^T J_v, g_v = J_v^T r_v and c_v = r_v^T r_v, from the residual
+ * d_r[n_voxels][n_points] and the tangents d_jz[n_tangents][n_voxels][n_points].
+ * d_H: [n_voxels][n_tangents][n_tangents], d_g: [n_voxels][n_tangents], d_c: [n_voxels].
+ */
+bmc_status bmc_normal_blocks(int32_t n_voxels, int32_t n_points, int32_t n_tangents,
+                             const double* d_r, const double* d_jz, double* d_H, double* d_g,
+                             double* d_c, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BMC_B200_H */
