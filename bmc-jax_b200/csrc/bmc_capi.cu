@@ -56,6 +56,12 @@ TaylorTable make_table(double tol, int m_max, double dense_theta, double dense_s
         }
         t.theta[m] = lo;
     }
+    double f = 1.0;
+    for (int k = 0; k <= kTaylorMMax; ++k) {
+        if (k > 0) f *= k;
+        t.inv_fact[k] = 1.0 / f;
+        t.inv_k[k] = k > 0 ? 1.0 / k : 0.0;
+    }
     t.dense_theta = dense_theta;
     int md = 1;
     while (md < kTaylorMMax && t.theta[md] < dense_theta) ++md;
@@ -85,7 +91,7 @@ bmc_status tables(int precision, const TaylorTable** out) {
     std::lock_guard<std::mutex> lk(g_mu);
     DeviceState& ds = dev_state(dev);
     if (!ds.tables_ready) {
-        TaylorTable h[2] = {make_table(std::ldexp(1.0, -53), 30, 0.5, 100.0),
+        TaylorTable h[2] = {make_table(1e-13, 30, 0.5, 100.0),
                             make_table(std::ldexp(1.0, -24), 16, 0.5, 100.0)};
         CUDA_TRY(cudaMemcpyToSymbol(g_tables, h, sizeof(h)));
         ds.tables_ready = true;
@@ -179,13 +185,34 @@ bmc_status prep_events(const bmc_problem* pr, const bmc_events* ev, EvRec<R>* ou
     return BMC_OK;
 }
 
+
+// ------------------------------------------------------------------------------------------------
+// FMA throughput probe: kChains independent fused multiply-add chains per thread, in registers
+// ------------------------------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(256) fma_probe_kernel(int iters, R seed, R* sink) {
+    constexpr int kChains = 8;
+    R a[kChains];
+#pragma unroll
+    for (int j = 0; j < kChains; ++j) a[j] = seed + R(threadIdx.x + j);
+    const R b = R(0.999999), c = R(1e-7);
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int j = 0; j < kChains; ++j) a[j] = fma(a[j], b, c);
+    }
+    R s = R(0);
+#pragma unroll
+    for (int j = 0; j < kChains; ++j) s += a[j];
+    if (s == R(-1.2345)) sink[blockIdx.x] = s;      // never true; keeps the loop alive
+}
+
 // ------------------------------------------------------------------------------------------------
 // launches
 // ------------------------------------------------------------------------------------------------
 template <int NC, typename R, int NT>
 bmc_status launch_chain(const ChainArgs& a, const TaylorTable* tt, cudaStream_t st) {
     constexpr int kWarps = 4;
-    const size_t smem = kWarps * sizeof(DenseSmem<NC, R, NT>);
+    const size_t smem = kWarps * sizeof(DenseSmem<NC, R, NT>) + 32 * kWarps * sizeof(ChainConst<NC, Dn<R, NT>>);
     CUDA_TRY(cudaFuncSetAttribute(chain_kernel<NC, R, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid = a.voxel_lanes ? dim3((a.n_vox + 127) / 128, a.n_off) : dim3((a.n_off + 127) / 128, a.n_vox);
     chain_kernel<NC, R, NT><<<grid, kWarps * 32, smem, st>>>(a, tt);
@@ -214,7 +241,7 @@ struct Impl {
     static constexpr int N = Layout<NC>::N;
 
     static bmc_status simulate(const bmc_problem* pr, const double* params, const bmc_events* ev, const double* m0,
-                               const bmc_spread* sp, double* out, cudaStream_t st) {
+                               const bmc_spread* sp, double* out, cudaStream_t st, unsigned long long* work = nullptr) {
         const TaylorTable* tt = nullptr;
         bmc_status s = tables(pr->precision, &tt);
         if (s != BMC_OK) return s;
@@ -227,7 +254,7 @@ struct Impl {
         a.n_vox = pr->n_voxels; a.n_off = pr->n_offsets; a.n_ev = pr->n_events; a.n_fields = Layout<NC>::NF;
         a.mz = pr->mz_loc; a.reset_after_adc = pr->reset_after_adc; a.voxel_lanes = voxel_lanes(pr) ? 1 : 0;
         if ((s = fill_spread(a, sp)) != BMC_OK) return s;
-        a.params = params; a.m0 = m0; a.out = out;
+        a.params = params; a.m0 = m0; a.out = out; a.work = work;
         a.status = cv.take<int>(1);
         CUDA_TRY(cudaMemsetAsync(a.status, 0, sizeof(int), st));
         if (pr->precision == BMC_F32) {
@@ -433,6 +460,15 @@ bmc_status bmc_simulate(const bmc_problem* prob, const double* d_params, const b
     BMC_DISPATCH(prob->n_cest, simulate(prob, d_params, ev, d_m0, spread, d_out, (cudaStream_t)stream));
 }
 
+bmc_status bmc_simulate_counted(const bmc_problem* prob, const double* d_params, const bmc_events* ev,
+                                const double* d_m0, const bmc_spread* spread, double* d_out,
+                                unsigned long long* d_work, void* stream) {
+    bmc_status s = check_problem(prob, d_params, ev, d_m0);
+    if (s != BMC_OK) return s;
+    if (!d_out || !d_work) return fail(BMC_ERR_INVALID, "null output or counters");
+    BMC_DISPATCH(prob->n_cest, simulate(prob, d_params, ev, d_m0, spread, d_out, (cudaStream_t)stream, d_work));
+}
+
 bmc_status bmc_simulate_trajectory(const bmc_problem* prob, const double* d_params, const bmc_events* ev,
                                    const double* d_m0, double* d_traj, void* stream) {
     bmc_status s = check_problem(prob, d_params, ev, d_m0);
@@ -492,6 +528,18 @@ bmc_status bmc_normal_blocks(int32_t n_voxels, int32_t n_points, int32_t n_tange
     normal_blocks_kernel<<<(n_voxels + 3) / 4, 128, 0, (cudaStream_t)stream>>>(n_voxels, n_points, n_tangents, d_r,
                                                                                d_jz, d_H, d_g, d_c);
     CUDA_TRY(cudaGetLastError());
+    return BMC_OK;
+}
+
+bmc_status bmc_probe_fma_peak(int32_t precision, int32_t blocks, int32_t iters, double* flops_per_launch,
+                              void* stream) {
+    if (blocks < 1 || iters < 1 || !flops_per_launch) return fail(BMC_ERR_INVALID, "probe: bad arguments");
+    if (precision == BMC_F32)
+        fma_probe_kernel<float><<<blocks, 256, 0, (cudaStream_t)stream>>>(iters, 1.0f, nullptr);
+    else
+        fma_probe_kernel<double><<<blocks, 256, 0, (cudaStream_t)stream>>>(iters, 1.0, nullptr);
+    CUDA_TRY(cudaGetLastError());
+    *flops_per_launch = 2.0 * 8.0 * 256.0 * (double)blocks * (double)iters;
     return BMC_OK;
 }
 

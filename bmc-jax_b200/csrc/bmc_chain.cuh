@@ -19,6 +19,8 @@ constexpr int kTaylorMMax = 40;
 // theta[m] = the largest ||X|| for which the degree-m tail bound stays under the tolerance.
 struct TaylorTable {
     double theta[kTaylorMMax + 1];
+    double inv_fact[kTaylorMMax + 1];   // 1 / k!
+    double inv_k[kTaylorMMax + 1];      // 1 / k
     int m_max;             // short path: degree cap
     double dense_theta;    // dense path: ||X / 2^s|| <= dense_theta ...
     int dense_m;           // ... with this Horner degree
@@ -46,6 +48,8 @@ struct ChainArgs {
     double* jout;              // [P][n_vox][n_off] or null
     double* traj;              // [n_vox][n_off][n_ev][N] or null: the state after every event
     int* status;               // error flags (bit 0: non-finite norm)
+    unsigned long long* work;  // null, or [4]: useful Taylor terms, dense Horner column products,
+                               // dense squarings, Taylor terms executed (warp maximum)
 };
 
 template <int NC>
@@ -240,20 +244,39 @@ struct Chain {
         for (int i = 0; i < NC; ++i) { t.xc[i] = a * t.xc[i]; t.yc[i] = a * t.yc[i]; t.zc[i] = a * t.zc[i]; }
     }
 
-    // exp(X)^s [M; 1] by s sub-steps of the degree-m Taylor polynomial; s applies to X already scaled
-    static __device__ __forceinline__ void taylor_apply(const StepCoef<NC, D>& s, int nsub, int m, State<NC, D>& M) {
-        for (int j = 0; j < nsub; ++j) {
+    // acc += a * t, entry by entry
+    static __device__ __forceinline__ void fma_state(State<NC, D>& acc, R a, const State<NC, D>& t) {
+        acc.xw = dfma(dconst<R, NT>(a), t.xw, acc.xw); acc.yw = dfma(dconst<R, NT>(a), t.yw, acc.yw);
+        acc.zw = dfma(dconst<R, NT>(a), t.zw, acc.zw); acc.zm = dfma(dconst<R, NT>(a), t.zm, acc.zm);
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+            acc.xc[i] = dfma(dconst<R, NT>(a), t.xc[i], acc.xc[i]);
+            acc.yc[i] = dfma(dconst<R, NT>(a), t.yc[i], acc.yc[i]);
+            acc.zc[i] = dfma(dconst<R, NT>(a), t.zc[i], acc.zc[i]);
+        }
+    }
+
+    // exp(X)^s [M; 1] by s sub-steps of the degree-m Taylor polynomial (X already scaled by the
+    // sub-step): the unnormalised powers p_k = X^k [M; 1] are accumulated with weights 1/k!, so each
+    // term is one sparse operator product and one fused multiply-add per state entry.
+    // The loops run to the warp's largest (s, m); each chain uses only its own (ns_own, m_own), so a
+    // chain's result never depends on which chains share its warp.
+    static __device__ __forceinline__ void taylor_apply(const StepCoef<NC, D>& s, int ns_w, int m_w, int ns_own,
+                                                        int m_own, State<NC, D>& M,
+                                                        const double* __restrict__ inv_fact) {
+#pragma unroll 1
+        for (int j = 0; j < ns_w; ++j) {
             State<NC, D> term, acc = M;
             matvec<true>(s, M, term);
             axpy_state(acc, term);
-            for (int k = 2; k <= m; ++k) {
+#pragma unroll 1
+            for (int k = 2; k <= m_w; ++k) {
                 State<NC, D> nt;
                 matvec<false>(s, term, nt);
-                scal_state(nt, R(1) / R(k));
                 term = nt;
-                axpy_state(acc, term);
+                fma_state(acc, k <= m_own ? R(inv_fact[k]) : R(0), term);
             }
-            M = acc;
+            if (j < ns_own) M = acc;
         }
     }
 

@@ -62,8 +62,9 @@ struct Dense {
             if (q == j) C::at(col, q) = dconst<R, NT>(R(1));
     }
 
-    static __device__ void event(SM* sm, int lane, bool evolve, const StepCoef<NC, D>& sc, R dt, R nu,
-                                 State<NC, D>& M, const TaylorTable& tt, int* status) {
+    static __device__ __noinline__ void event(SM* sm, int lane, bool evolve, const StepCoef<NC, D>& sc, R dt, R nu,
+                                 State<NC, D>& M, const TaylorTable& tt, int* status, bool count,
+                                 unsigned long long& wh, unsigned long long& ws) {
         unsigned need = __ballot_sync(kFull, evolve);
         while (need) {
             const int c = __ffs(need) - 1;
@@ -79,6 +80,10 @@ struct Dense {
                 C::scale_coef(scs, R(ldexp(double(dt), -s)));
                 sm->coef = scs;
                 sm->s = s;
+                if (count) {
+                    wh += (unsigned long long)NA * tt.dense_m;
+                    ws += (unsigned long long)s;
+                }
 #pragma unroll
                 for (int q = 0; q < N; ++q) sm->vec[q] = C::at(M, q);
                 sm->vec[N] = dconst<R, NT>(R(1));
@@ -93,7 +98,7 @@ struct Dense {
                 for (int k = tt.dense_m; k >= 1; --k) {
                     State<NC, D> y;
                     matvec_aug(sm->coef, col, caug, y);
-                    C::scal_state(y, R(1) / R(k));
+                    C::scal_state(y, R(tt.inv_k[k]));
                     State<NC, D> e;
                     unit(e, lane);
                     C::axpy_state(e, y);
@@ -150,7 +155,7 @@ struct Dense {
 // the chain kernel
 // ------------------------------------------------------------------------------------------------
 template <int NC, typename R, int NT>
-__global__ void __launch_bounds__(128) chain_kernel(const ChainArgs a, const TaylorTable* __restrict__ ttab) {
+__global__ void __launch_bounds__(128, 2) chain_kernel(const ChainArgs a, const TaylorTable* __restrict__ ttab) {
     using D = Dn<R, NT>;
     using C = Chain<NC, R, NT>;
     using SM = DenseSmem<NC, R, NT>;
@@ -177,9 +182,15 @@ __global__ void __launch_bounds__(128) chain_kernel(const ChainArgs a, const Tay
     const EvRec<R>* __restrict__ ev = reinterpret_cast<const EvRec<R>*>(a.ev);
 
     const size_t ch = (size_t)v * a.n_off + o;
+    unsigned long long wk0 = 0, wk1 = 0, wk2 = 0, wk3 = 0;
+    const bool count = a.work != nullptr;
+    ChainConst<NC, D>& cc = reinterpret_cast<ChainConst<NC, D>*>(smem_raw + 4 * sizeof(SM))[threadIdx.x];
     for (int node = 0; node < a.n_nodes; ++node) {
-        ChainConst<NC, D> cc;
-        C::load_const(a, v, node, cc);
+        {
+            ChainConst<NC, D> tmp;
+            C::load_const(a, v, node, tmp);
+            cc = tmp;
+        }
         State<NC, D> M;
         C::load_m0(a, v, M);
         bool reset_pending = false;
@@ -211,19 +222,27 @@ __global__ void __launch_bounds__(128) chain_kernel(const ChainArgs a, const Tay
                     if (evolve) atomicOr(a.status, 1);
                     nu = R(0);
                 }
-                const R numax = warp_max(nu);
-                if (numax > R(tt.dense_switch)) {
-                    Dense<NC, R, NT>::event(dsm, lane, evolve, sc, rec.dt, nu, M, tt, a.status);
-                } else if (numax > R(0)) {
-                    int m = 1, nsub = 1;
+                // this chain's own choice: dense scaling and squaring for a large norm, else the
+                // Taylor action with the fewest terms whose tail bound meets the tolerance
+                const bool dense_own = evolve && nu > R(tt.dense_switch);
+                if (__any_sync(kFull, dense_own))
+                    Dense<NC, R, NT>::event(dsm, lane, dense_own, sc, rec.dt, nu, M, tt, a.status, count, wk1, wk2);
+                const bool tay = evolve && !dense_own;
+                int m_own = 0, ns_own = 0;
+                if (tay) {
                     const R thm = R(tt.theta[tt.m_max]);
-                    if (numax > thm) nsub = (int)ceil(numax / thm);
-                    const R per = numax / R(nsub);
-                    while (m < tt.m_max && R(tt.theta[m]) < per) ++m;
-                    C::scale_coef(sc, rec.dt / R(nsub));
-                    State<NC, D> Mn = M;
-                    C::taylor_apply(sc, nsub, m, Mn);
-                    if (evolve) M = Mn;
+                    ns_own = nu > thm ? (int)ceil(nu / thm) : 1;
+                    const R per = nu / R(ns_own);
+                    m_own = 1;
+                    while (m_own < tt.m_max && R(tt.theta[m_own]) < per) ++m_own;
+                }
+                const int ns_w = __reduce_max_sync(kFull, (unsigned)ns_own);
+                const int m_w = __reduce_max_sync(kFull, (unsigned)m_own);
+                if (ns_w > 0) {
+                    C::scale_coef(sc, tay ? rec.dt / R(ns_own) : R(0));
+                    C::taylor_apply(sc, ns_w, m_w, ns_own, m_own, M, tt.inv_fact);
+                    if (count && tay) wk0 += (unsigned long long)ns_own * m_own;
+                    if (count) wk3 += (unsigned long long)ns_w * m_w;
                 }
             }
             if (type == EV_GRADIENT || type == EV_SPOILER) C::spoil(M);
@@ -257,6 +276,15 @@ __global__ void __launch_bounds__(128) chain_kernel(const ChainArgs a, const Tay
                 for (int q = 0; q < N; ++q)
                     a.out[ch * N + q] = (node ? a.out[ch * N + q] : 0.0) + double(wgt * C::at(M, q).v);
             }
+        }
+    }
+    if (a.work) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            unsigned long long x = act ? (q == 0 ? wk0 : (q == 1 ? wk1 : (q == 2 ? wk2 : wk3))) : 0ull;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(kFull, x, off);
+            if (lane == 0 && x) atomicAdd(a.work + q, x);
         }
     }
 }

@@ -173,6 +173,21 @@ bmc_status bmc_normal_blocks(int32_t n_voxels, int32_t n_points, int32_t n_tange
                              const double* d_r, const double* d_jz, double* d_H, double* d_g,
                              double* d_c, void* stream);
 
+/*
+ * Diagnostics (no counterpart in the reference: measurement support for the benchmark).
+ * bmc_simulate_counted: bmc_simulate that also adds the work it executed to d_work[4] (device,
+ *   zeroed by the caller): [0] Taylor sub-step terms each chain needed (one sparse operator product
+ *   each), [1] dense-path Horner column products, [2] dense-path squarings, [3] Taylor terms executed
+ *   (a warp runs to the largest need among its chains).
+ * bmc_probe_fma_peak: launches `blocks` x 256 threads of 8 independent FMA chains x `iters`
+ *   (float64 or float32) and returns the FLOPs one launch executes, to time against.
+ */
+bmc_status bmc_simulate_counted(const bmc_problem* prob, const double* d_params, const bmc_events* ev,
+                                const double* d_m0, const bmc_spread* spread, double* d_out,
+                                unsigned long long* d_work, void* stream);
+bmc_status bmc_probe_fma_peak(int32_t precision, int32_t blocks, int32_t iters, double* flops_per_launch,
+                              void* stream);
+
 #ifdef __cplusplus
 }
 #endif

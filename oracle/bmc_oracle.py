@@ -536,3 +536,40 @@ def fit_voxel(p: Params, ev: Events, M0, slots, z_meas, x0_phys, lo_phys, hi_phy
         x, X, C = out
         return x * sc, X * sc[None, :], C
     return out * sc
+
+
+# ------------------------------------------------------------------------------------------------
+# the C twin (oracle/bmc_oracle.c): same algorithm family, compiled, OpenMP over chains
+# ------------------------------------------------------------------------------------------------
+def c_oracle():
+    """ctypes handle of oracle/_build/liboracle.so (built on demand with gcc)."""
+    import ctypes as C
+    from pathlib import Path
+    here = Path(__file__).resolve().parent
+    so = here / "_build" / "liboracle.so"
+    if not so.exists():
+        import subprocess, sys
+        subprocess.run([sys.executable, str(here / "build.py")], check=True)
+    L = C.CDLL(str(so))
+    d, i = C.POINTER(C.c_double), C.POINTER(C.c_int)
+    L.oracle_simulate.argtypes = [C.c_int] * 4 + [d, i, d, d, d, d, d, C.c_int, d, C.c_int]
+    L.oracle_simulate.restype = C.c_int
+    L.oracle_threads.restype = C.c_int
+    return L
+
+
+def c_simulate_z(params_soa, ev: Events, m0, n_cest, mz, threads=0):
+    """Z[v][o] from the C oracle. params_soa: [13 + 5 n_cest][n_vox] float64 (the C ABI layout)."""
+    import ctypes as C
+    L = c_oracle()
+    P = np.ascontiguousarray(params_soa, np.float64)
+    nv = P.shape[1]
+    n_off, n_ev = np.shape(ev.dt)
+    t = np.ascontiguousarray(ev.type, np.int32)
+    arr = [np.ascontiguousarray(getattr(ev, f), np.float64) for f in ("dt", "rf_amp", "rf_phase", "rf_freq")]
+    m = np.ascontiguousarray(np.broadcast_to(np.asarray(m0, np.float64), (nv, state_size(n_cest))))
+    out = np.empty((nv, n_off))
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    L.oracle_simulate(nv, n_off, n_ev, n_cest, dp(P), t.ctypes.data_as(C.POINTER(C.c_int)), *[dp(a) for a in arr],
+                      dp(m), int(mz), dp(out), int(threads))
+    return out

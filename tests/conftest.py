@@ -8,6 +8,7 @@ import pytest
 ROOT = Path(__file__).resolve().parents[1]
 sys.path.insert(0, str(ROOT / "bmc-jax_b200"))
 sys.path.insert(0, str(ROOT / "oracle"))
+sys.path.insert(0, str(ROOT))
 GOLDEN = ROOT / "tests" / "golden"
 
 

@@ -115,3 +115,16 @@ def test_readme_quick_start_fit_is_recovered():
     np.testing.assert_allclose(x, d["readme_x"][0], rtol=1e-5)
     np.testing.assert_allclose(d["readme_x"][0], [50.0, 9.009e-4], rtol=1e-6)
     assert abs(49.617 / x[0] - 1) < 0.01 and abs(9.0772e-4 / x[1] - 1) < 0.01
+
+
+@pytest.mark.parametrize("tag", SPECTRA + ["quesp"])
+def test_c_oracle_matches_the_reference(tag):
+    """The compiled twin (oracle/bmc_oracle.c, Pade-13 scaling and squaring) on every golden case."""
+    d = golden("spectra")
+    p = unpack_params(d, f"{tag}_p_", O.Params)
+    ev = unpack_events(d, f"{tag}_e_", O.Events)
+    nc = O.n_cest_of(p)
+    mz = int(d[f"{tag}_mz"])
+    from bmc_b200.simulation import pack_params, SimParams
+    z = O.c_simulate_z(pack_params(SimParams(*p), 1), ev, d[f"{tag}_m0"], nc, mz)
+    np.testing.assert_allclose(z[0], d[f"{tag}_M"][:, mz], rtol=0, atol=1e-10)
