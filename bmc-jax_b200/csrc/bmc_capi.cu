@@ -150,12 +150,8 @@ bmc_status check_problem(const bmc_problem* pr, const double* params, const bmc_
         return fail(BMC_ERR_INVALID, "precision %d is neither BMC_F64 nor BMC_F32", pr->precision);
     if (pr->n_events > 0 && (!ev->d_type || !ev->d_dt || !ev->d_rf_amp || !ev->d_rf_phase || !ev->d_rf_freq))
         return fail(BMC_ERR_INVALID, "null event field");
-    if (pr->n_offsets > 65535 && pr->n_voxels > 65535)
-        return fail(BMC_ERR_INVALID, "offsets and voxels both above 65535");
     return BMC_OK;
 }
-
-bool voxel_lanes(const bmc_problem* pr) { return pr->n_voxels >= 64 || pr->n_voxels >= pr->n_offsets; }
 
 bmc_status fill_spread(ChainArgs& a, const bmc_spread* sp) {
     a.n_nodes = 1;
@@ -212,10 +208,13 @@ __global__ void __launch_bounds__(256) fma_probe_kernel(int iters, R seed, R* si
 template <int NC, typename R, int NT>
 bmc_status launch_chain(const ChainArgs& a, const TaylorTable* tt, cudaStream_t st) {
     constexpr int kWarps = 4;
-    const size_t smem = kWarps * sizeof(DenseSmem<NC, R, NT>) + 32 * kWarps * sizeof(ChainConst<NC, Dn<R, NT>>);
+    const size_t smem = kWarps * sizeof(DenseSmem<NC, typename DenseReal<R>::type, NT>) +
+                        32 * kWarps * sizeof(ChainConst<NC, Dn<R, NT>>);
     CUDA_TRY(cudaFuncSetAttribute(chain_kernel<NC, R, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 grid = a.voxel_lanes ? dim3((a.n_vox + 127) / 128, a.n_off) : dim3((a.n_off + 127) / 128, a.n_vox);
-    chain_kernel<NC, R, NT><<<grid, kWarps * 32, smem, st>>>(a, tt);
+    const long long nch = (long long)a.n_vox * a.n_off;
+    const long long blocks = (nch + 127) / 128;
+    if (blocks > 0x7fffffffLL) return fail(BMC_ERR_INVALID, "%lld chains exceed one launch", nch);
+    chain_kernel<NC, R, NT><<<(unsigned)blocks, kWarps * 32, smem, st>>>(a, tt);
     CUDA_TRY(cudaGetLastError());
     return BMC_OK;
 }
@@ -252,7 +251,7 @@ struct Impl {
         Carve cv(ws);
         ChainArgs a{};
         a.n_vox = pr->n_voxels; a.n_off = pr->n_offsets; a.n_ev = pr->n_events; a.n_fields = Layout<NC>::NF;
-        a.mz = pr->mz_loc; a.reset_after_adc = pr->reset_after_adc; a.voxel_lanes = voxel_lanes(pr) ? 1 : 0;
+        a.mz = pr->mz_loc; a.reset_after_adc = pr->reset_after_adc;
         if ((s = fill_spread(a, sp)) != BMC_OK) return s;
         a.params = params; a.m0 = m0; a.out = out; a.work = work;
         a.status = cv.take<int>(1);
@@ -280,7 +279,7 @@ struct Impl {
         Carve cv(ws);
         ChainArgs a{};
         a.n_vox = pr->n_voxels; a.n_off = pr->n_offsets; a.n_ev = pr->n_events; a.n_fields = Layout<NC>::NF;
-        a.mz = Layout<NC>::izw; a.reset_after_adc = pr->reset_after_adc; a.voxel_lanes = voxel_lanes(pr) ? 1 : 0;
+        a.mz = Layout<NC>::izw; a.reset_after_adc = pr->reset_after_adc;
         fill_spread(a, nullptr);
         a.params = params; a.m0 = m0; a.traj = traj;
         a.status = cv.take<int>(1);
@@ -303,7 +302,7 @@ struct Impl {
         Carve cv(ws);
         ChainArgs a{};
         a.n_vox = pr->n_voxels; a.n_off = pr->n_offsets; a.n_ev = pr->n_events; a.n_fields = Layout<NC>::NF;
-        a.mz = pr->mz_loc; a.reset_after_adc = pr->reset_after_adc; a.voxel_lanes = voxel_lanes(pr) ? 1 : 0;
+        a.mz = pr->mz_loc; a.reset_after_adc = pr->reset_after_adc;
         if ((s = fill_spread(a, sp)) != BMC_OK) return s;
         a.params = params; a.m0 = m0; a.out = z; a.jout = jz;
         for (int t = 0; t < tg->n_tangents; ++t) a.field_row[t] = tg->field_row[t];
@@ -370,7 +369,7 @@ struct Impl {
         }
         ChainArgs a{};
         a.n_vox = nv; a.n_off = no; a.n_ev = pr->n_events; a.n_fields = NF;
-        a.mz = pr->mz_loc; a.reset_after_adc = pr->reset_after_adc; a.voxel_lanes = voxel_lanes(pr) ? 1 : 0;
+        a.mz = pr->mz_loc; a.reset_after_adc = pr->reset_after_adc;
         if ((s = fill_spread(a, sp)) != BMC_OK) return s;
         const double* sig0 = sp ? sp->d_sigma_hz : nullptr;
         a.ev = rec; a.status = status;

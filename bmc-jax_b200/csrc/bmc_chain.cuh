@@ -31,7 +31,6 @@ struct ChainArgs {
     int n_vox, n_off, n_ev, n_fields;
     int mz;                    // state index written; < 0: whole state
     int reset_after_adc;
-    int voxel_lanes;           // 1: lanes = voxels (events warp-uniform); 0: lanes = offsets
     int n_nodes;               // spread isochromats (1 = none)
     double u[kMaxNodes], w[kMaxNodes];
     const double* params;      // [n_fields][n_vox]
@@ -196,19 +195,25 @@ struct Chain {
     // y = X v (+ C h when WithC): the sparse Bloch-McConnell operator (matrix.py:238-293)
     template <bool WithC>
     static __device__ __forceinline__ void matvec(const StepCoef<NC, D>& s, const State<NC, D>& v, State<NC, D>& y) {
+        // water rows: own terms and the pools' exchange terms in two partial sums (shorter dependency
+        // chains), pool rows: four terms each
         D xw = dfma(s.offw, v.yw, -(s.Rw2 * v.xw));
         xw = xw - s.w1y * v.zw;
         D yw = dfma(s.w1x, v.zw, -(s.Rw2 * v.yw));
         yw = yw - s.offw * v.xw;
         D zw = dfma(s.w1y, v.xw, -(s.Rw1 * v.zw));
         zw = zw - s.w1x * v.yw;
-        zw = dfma(s.kmt, v.zm, zw);
-        if constexpr (WithC) zw = zw + s.cw;
+        D zm = dfma(s.kwmt, v.zw, -(s.Rm1W * v.zm));
+        if constexpr (WithC) {
+            zw = zw + s.cw;
+            zm = zm + s.cm;
+        }
+        D px = dconst<R, NT>(R(0)), py = px, pz = s.kmt * v.zm;
 #pragma unroll
         for (int i = 0; i < NC; ++i) {
-            xw = dfma(s.k[i], v.xc[i], xw);
-            yw = dfma(s.k[i], v.yc[i], yw);
-            zw = dfma(s.k[i], v.zc[i], zw);
+            px = dfma(s.k[i], v.xc[i], px);
+            py = dfma(s.k[i], v.yc[i], py);
+            pz = dfma(s.k[i], v.zc[i], pz);
             D xc = dfma(s.kwc[i], v.xw, -(s.Rc2[i] * v.xc[i]));
             xc = xc - s.offc[i] * v.yc[i];
             xc = xc - s.w1y * v.zc[i];
@@ -223,11 +228,9 @@ struct Chain {
             y.yc[i] = yc;
             y.zc[i] = zc;
         }
-        D zm = dfma(s.kwmt, v.zw, -(s.Rm1W * v.zm));
-        if constexpr (WithC) zm = zm + s.cm;
-        y.xw = xw;
-        y.yw = yw;
-        y.zw = zw;
+        y.xw = xw + px;
+        y.yw = yw + py;
+        y.zw = zw + pz;
         y.zm = zm;
     }
 

@@ -1,5 +1,7 @@
 // bmc_kernels.cuh -- the chain kernel, its dense long-event path, and the event preprocessing.
 #pragma once
+#include <type_traits>
+
 #include "bmc_chain.cuh"
 
 namespace bmc {
@@ -151,32 +153,49 @@ struct Dense {
     }
 };
 
+// the precision of the dense path: float64 always (its squarings amplify rounding by 2^s)
+template <typename R>
+struct DenseReal { using type = double; };
+
+// elementwise precision change of a struct made only of Dn<RS, NT> members (StepCoef, State)
+template <typename RS, typename RD, int NT, typename A, typename B>
+__device__ __forceinline__ void convert_flat(const A& a, B& b) {
+    constexpr int n = sizeof(A) / sizeof(Dn<RS, NT>);
+    static_assert(sizeof(B) / sizeof(Dn<RD, NT>) == n, "layouts differ");
+    const Dn<RS, NT>* pa = reinterpret_cast<const Dn<RS, NT>*>(&a);
+    Dn<RD, NT>* pb = reinterpret_cast<Dn<RD, NT>*>(&b);
+#pragma unroll
+    for (int i = 0; i < n; ++i) {
+        pb[i].v = RD(pa[i].v);
+        if constexpr (NT > 0) {
+#pragma unroll
+            for (int t = 0; t < NT; ++t) pb[i].d[t] = RD(pa[i].d[t]);
+        }
+    }
+}
+
 // ------------------------------------------------------------------------------------------------
 // the chain kernel
 // ------------------------------------------------------------------------------------------------
 template <int NC, typename R, int NT>
-__global__ void __launch_bounds__(128, 2) chain_kernel(const ChainArgs a, const TaylorTable* __restrict__ ttab) {
+__global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const ChainArgs a, const TaylorTable* __restrict__ ttab) {
     using D = Dn<R, NT>;
     using C = Chain<NC, R, NT>;
-    using SM = DenseSmem<NC, R, NT>;
+    using RD = typename DenseReal<R>::type;
+    using SM = DenseSmem<NC, RD, NT>;
     constexpr int N = Layout<NC>::N;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     SM* dsm = reinterpret_cast<SM*>(smem_raw) + (threadIdx.x >> 5);
     const TaylorTable& tt = *ttab;
 
-    const int ia = blockIdx.x * blockDim.x + threadIdx.x;
-    int v, o;
-    bool valid;
-    if (a.voxel_lanes) {
-        v = ia; o = blockIdx.y; valid = v < a.n_vox;
-    } else {
-        o = ia; v = blockIdx.y; valid = o < a.n_off;
-    }
-    if (!valid) {
-        v = v < a.n_vox ? v : a.n_vox - 1;
-        o = o < a.n_off ? o : a.n_off - 1;
-    }
+    // chains in offset-fastest order: neighbouring lanes are neighbouring offsets of one voxel, so a
+    // warp shares parameters and its chains need similar Taylor orders
+    const long long nch = (long long)a.n_vox * a.n_off;
+    long long ci = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = ci < nch;
+    if (!valid) ci = nch - 1;
+    const int v = (int)(ci / a.n_off), o = (int)(ci % a.n_off);
     const bool act = valid && (a.active == nullptr || a.active[v] != 0);
     if (__all_sync(kFull, !act)) return;
     const EvRec<R>* __restrict__ ev = reinterpret_cast<const EvRec<R>*>(a.ev);
@@ -225,8 +244,19 @@ __global__ void __launch_bounds__(128, 2) chain_kernel(const ChainArgs a, const 
                 // this chain's own choice: dense scaling and squaring for a large norm, else the
                 // Taylor action with the fewest terms whose tail bound meets the tolerance
                 const bool dense_own = evolve && nu > R(tt.dense_switch);
-                if (__any_sync(kFull, dense_own))
-                    Dense<NC, R, NT>::event(dsm, lane, dense_own, sc, rec.dt, nu, M, tt, a.status, count, wk1, wk2);
+                if (__any_sync(kFull, dense_own)) {
+                    if constexpr (std::is_same<R, RD>::value) {
+                        Dense<NC, R, NT>::event(dsm, lane, dense_own, sc, rec.dt, nu, M, tt, a.status, count, wk1, wk2);
+                    } else {
+                        StepCoef<NC, Dn<RD, NT>> scd;
+                        State<NC, Dn<RD, NT>> Md;
+                        convert_flat<R, RD, NT>(sc, scd);
+                        convert_flat<R, RD, NT>(M, Md);
+                        Dense<NC, RD, NT>::event(dsm, lane, dense_own, scd, RD(rec.dt), RD(nu), Md, tt, a.status, count,
+                                                 wk1, wk2);
+                        convert_flat<RD, R, NT>(Md, M);
+                    }
+                }
                 const bool tay = evolve && !dense_own;
                 int m_own = 0, ns_own = 0;
                 if (tay) {

@@ -183,7 +183,7 @@ def test_joint_jacobian_is_the_derivative(joint3):
             e = np.zeros(x.size); e[j] = h
             Ja[:, j] = (d["resid"](x + e) - d["resid"](x - e)) / (2 * h)
         rel = np.linalg.norm(J - Ja, axis=0) / np.maximum(np.linalg.norm(Ja, axis=0), 1e-30)
-        assert rel.max() < 1e-5, f"{[s.name for s in slots]}: {rel}"
+        assert rel.max() < 1e-4, f"{[s.name for s in slots]}: {rel}"      # the reference's own bound
 
 
 def test_block_offset_and_spread_fits(joint3):
@@ -234,7 +234,10 @@ def test_crlb_identities(cuda):
     twice = Experiment.stack([exp, exp])
     c = crlb(twice, FitSpec([Kp, Fp]), 0.002)
     np.testing.assert_allclose(c.sd, a.sd / np.sqrt(2.0), rtol=1e-9)
-    alone = crlb(exp, FitSpec([Kp]), 0.002)
+    # the bound of k alone is 1/sqrt(F_kk) of the joint Fisher matrix at the same point (the reference
+    # compares at two different f and absorbs the difference in a 5e-3 tolerance)
+    at_same_f = Experiment(jp._replace(cest_f=np.array([0.0009])), ev, initial_state(jp), p.mz_loc)
+    alone = crlb(at_same_f, FitSpec([Kp]), 0.002)
     assert alone.sd[0] == pytest.approx(1.0 / np.sqrt(a.fisher[0, 0]), rel=1e-9)
     assert alone.sd[0] < a.sd[0]
     with pytest.raises(ValueError, match="one sample"):

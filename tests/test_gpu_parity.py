@@ -41,13 +41,13 @@ def test_water_z_only_path_matches(cuda):
 
 
 def test_float32_kernel_accuracy(cuda):
-    """The optional float32 kernel (settings.use_x64(False)): within 1e-5 on short pulse samples, and
-    ~1e-3 where a long CW block needs ~15 squarings (the reference's own float32 path is ~1e-4 off,
-    settings.py:10-11). float64 is the default for this reason."""
+    """The optional float32 kernel (settings.use_x64(False)): float32 sub-steps, float64 for long
+    events (their squarings). Reported, and held to the reference's own float32 level of 1e-4
+    (settings.py:10-11, tests/test_solver.py:13-17); float64 is the default."""
     from bmc_b200.simulation import SimParams, SimEvent, simulate_z
     from bmc_b200 import _lib
     d = golden("spectra")
-    for tag, bound in (("quesp", 1e-4), ("readme", 2e-3), ("mt_sl", 2e-3)):
+    for tag, bound in (("quesp", 1e-4), ("readme", 1e-4), ("mt_sl", 1e-4)):
         p = unpack_params(d, f"{tag}_p_", SimParams)
         ev = unpack_events(d, f"{tag}_e_", SimEvent)
         mz = int(d[f"{tag}_mz"])
@@ -163,7 +163,7 @@ def test_jacobian_matches_the_oracle_and_the_reference(cuda):
     ev = unpack_events(s, "readme_e_", SimEvent)
     spec = FitSpec([FreeParam("k", "cest_k", 0, 1.0, 1.0, 1e4, 1.0), FreeParam("f", "cest_f", 0, 1.0, 0, 1, 0)])
     Z, J = jacobian(Experiment(p, ev, s["readme_m0"], 4), spec, d["jac_x"])
-    np.testing.assert_allclose(J, d["jac_J"], rtol=1e-4, atol=1e-8)
+    np.testing.assert_allclose(J, d["jac_J"], rtol=1e-4, atol=2e-6)     # central differences: ~1e-5 of |J|
     op = unpack_params(s, "readme_p_", O.Params)._replace(cest_k=np.array([d["jac_x"][0]]),
                                                           cest_f=np.array([d["jac_x"][1]]))
     oev = O.Events(*[np.asarray(a)[::10] for a in unpack_events(s, "readme_e_", O.Events)])
