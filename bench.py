@@ -127,6 +127,22 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def max_over_ranks(x: float, device=None) -> float:
+    """The largest value of x over every rank (the step time of the slowest GPU); x itself alone."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rank_seed(rank: int) -> int:
+    """Every rank simulates its own voxels (weak scaling): distinct seeds per rank."""
+    return 1000 + rank
+
+
 def measured_peaks():
     try:
         return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
@@ -173,7 +189,7 @@ def run_ours(args, rank, world, local_rank):
     nc = args.pools
     N = 3 * (1 + nc) + 1
     mz = 2 * (1 + nc)
-    P, M0 = voxel_params(args.voxels, nc, seed=1000 + rank)
+    P, M0 = voxel_params(args.voxels, nc, seed=rank_seed(rank))
     ev = pulse_train(args.offsets, n_pulses=args.pulses)
     n_off, n_ev = ev[0].shape
     nv = args.voxels
@@ -228,11 +244,8 @@ def run_ours(args, rank, world, local_rank):
         times.append(e0.elapsed_time(e1))
     torch.cuda.synchronize(dev)
     clocks = sampler.stop()
-    ms = float(np.mean(times))
+    ms = max_over_ranks(float(np.mean(times)), dev)
     if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
 
     # end to end: host buffers in, Z back to the host, copies inside the timed region
@@ -250,11 +263,7 @@ def run_ours(args, rank, world, local_rank):
         e1.record(stream)
         e1.synchronize()
         e2e.append(e0.elapsed_time(e1))
-    e2e_ms = float(np.mean(e2e))
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(float(np.mean(e2e)), dev)
     h2d = sum(x.numel() * x.element_size() for x in [hP, hM] + hev)
     d2h = hZ.numel() * hZ.element_size()
 

@@ -15,6 +15,8 @@
 #include <vector>
 
 #include "../../include/bmc_b200.h"
+#include <cub/device/device_radix_sort.cuh>
+
 #include "bmc_lm.cuh"
 
 using namespace bmc;
@@ -219,6 +221,34 @@ bmc_status launch_chain(const ChainArgs& a, const TaylorTable* tt, cudaStream_t 
     return BMC_OK;
 }
 
+// Order the chains by estimated cost: `order` and the sort's scratch are carved from `cv`.
+template <int NC, typename R>
+bmc_status order_chains(ChainArgs& a, Carve& cv, cudaStream_t st) {
+    const long long nch = (long long)a.n_vox * a.n_off;
+    if (nch < 2 * 128 || a.n_ev == 0) return BMC_OK;
+    float* k_in = cv.take<float>(nch);
+    float* k_out = cv.take<float>(nch);
+    int* i_in = cv.take<int>(nch);
+    int* i_out = cv.take<int>(nch);
+    size_t tmp = 0;
+    CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp, k_in, k_out, i_in, i_out, (int)nch, 0, 32, st));
+    void* t = cv.take<char>(tmp);
+    cost_kernel<NC, R><<<(unsigned)((nch + 127) / 128), 128, 0, st>>>(a, k_in, i_in);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cub::DeviceRadixSort::SortPairs(t, tmp, k_in, k_out, i_in, i_out, (int)nch, 0, 32, st));
+    a.order = i_out;
+    return BMC_OK;
+}
+
+// scratch bytes order_chains carves for n chains
+size_t order_bytes(long long nch) {
+    size_t tmp = 0;
+    float* f = nullptr;
+    int* i = nullptr;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp, f, f, i, i, (int)std::max<long long>(nch, 1), 0, 32);
+    return 4 * align256(sizeof(float) * nch) + align256(tmp) + 1024;
+}
+
 // tangents per launch, by pool count (register budget of the dual-number state)
 template <int NC>
 constexpr int tangents_per_pass() { return NC <= 1 ? 2 : 1; }
@@ -247,7 +277,8 @@ struct Impl {
         const size_t nrec = (size_t)pr->n_offsets * pr->n_events;
         void* ws = nullptr;
         const size_t recb = pr->precision == BMC_F32 ? sizeof(EvRec<float>) : sizeof(EvRec<double>);
-        if ((s = workspace(align256(nrec * recb) + 256, &ws)) != BMC_OK) return s;
+        const long long nch = (long long)pr->n_voxels * pr->n_offsets;
+        if ((s = workspace(align256(nrec * recb) + 256 + order_bytes(nch), &ws)) != BMC_OK) return s;
         Carve cv(ws);
         ChainArgs a{};
         a.n_vox = pr->n_voxels; a.n_off = pr->n_offsets; a.n_ev = pr->n_events; a.n_fields = Layout<NC>::NF;
@@ -260,11 +291,13 @@ struct Impl {
             EvRec<float>* rec = cv.take<EvRec<float>>(nrec);
             if ((s = prep_events<float>(pr, ev, rec, st)) != BMC_OK) return s;
             a.ev = rec;
+            if ((s = order_chains<NC, float>(a, cv, st)) != BMC_OK) return s;
             return launch_chain<NC, float, 0>(a, tt, st);
         }
         EvRec<double>* rec = cv.take<EvRec<double>>(nrec);
         if ((s = prep_events<double>(pr, ev, rec, st)) != BMC_OK) return s;
         a.ev = rec;
+        if ((s = order_chains<NC, double>(a, cv, st)) != BMC_OK) return s;
         return launch_chain<NC, double, 0>(a, tt, st);
     }
 
@@ -298,7 +331,8 @@ struct Impl {
         if (s != BMC_OK) return s;
         const size_t nrec = (size_t)pr->n_offsets * pr->n_events;
         void* ws = nullptr;
-        if ((s = workspace(align256(nrec * sizeof(EvRec<double>)) + 256, &ws)) != BMC_OK) return s;
+        const long long nch = (long long)pr->n_voxels * pr->n_offsets;
+        if ((s = workspace(align256(nrec * sizeof(EvRec<double>)) + 256 + order_bytes(nch), &ws)) != BMC_OK) return s;
         Carve cv(ws);
         ChainArgs a{};
         a.n_vox = pr->n_voxels; a.n_off = pr->n_offsets; a.n_ev = pr->n_events; a.n_fields = Layout<NC>::NF;
@@ -312,6 +346,7 @@ struct Impl {
         EvRec<double>* rec = cv.take<EvRec<double>>(nrec);
         if ((s = prep_events<double>(pr, ev, rec, st)) != BMC_OK) return s;
         a.ev = rec;
+        if ((s = order_chains<NC, double>(a, cv, st)) != BMC_OK) return s;
         return run_tangents<NC>(a, tg->n_tangents, tt, st);
     }
 
@@ -329,7 +364,7 @@ struct Impl {
                              align256(sizeof(double) * P * nv) + align256(sizeof(double) * P * nv * N) +
                              2 * align256(sizeof(double) * nv * no) + align256(sizeof(double) * P * nv * no) +
                              2 * align256(sizeof(double) * nv * P) + 2 * align256(sizeof(double) * nv) +
-                             align256(sizeof(int) * nv) + 4096;
+                             align256(sizeof(int) * nv) + 4096 + order_bytes((long long)nv * no);
         void* ws = nullptr;
         if ((s = workspace(bytes, &ws)) != BMC_OK) return s;
         Carve cv(ws);
@@ -373,6 +408,8 @@ struct Impl {
         if ((s = fill_spread(a, sp)) != BMC_OK) return s;
         const double* sig0 = sp ? sp->d_sigma_hz : nullptr;
         a.ev = rec; a.status = status;
+        a.params = params; a.m0 = m0;
+        if ((s = order_chains<NC, double>(a, cv, st)) != BMC_OK) return s;
         for (int p = 0; p < P; ++p) a.field_row[p] = fs->field_row[p] == BMC_SLOT_M_START ? BMC_SEED_NONE : fs->field_row[p];
         const int vb = (nv + 127) / 128, wb = (nv + 3) / 4;
         for (int it = 0; it < fs->n_iter; ++it) {

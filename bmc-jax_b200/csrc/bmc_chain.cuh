@@ -43,6 +43,7 @@ struct ChainArgs {
     const double* seed;        // [P][n_vox]
     const double* dm0;         // [P][n_vox][N] or null
     const int* active;         // [n_vox] or null: voxels with 0 are skipped
+    const int* order;          // [n_vox * n_off] or null: the chain each thread takes, in launch order
     double* out;               // [n_vox][n_off] (mz >= 0) or [n_vox][n_off][N]
     double* jout;              // [P][n_vox][n_off] or null
     double* traj;              // [n_vox][n_off][n_ev][N] or null: the state after every event
@@ -134,6 +135,13 @@ struct Chain {
         int ls = (int)a.params[(size_t)L::MLS * a.n_vox + v];
         cc.ls = ls < 0 ? 0 : (ls > 2 ? 2 : ls);
         cc.mt_on = fmt.v > R(1e-9);
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+            const double f = a.params[(size_t)(L::CF + i) * a.n_vox + v];
+            cc.sf[i] = f > 1e-30 ? sqrt(f) : 1.0;
+        }
+        const double fm = a.params[(size_t)L::MF * a.n_vox + v];
+        cc.sfm = fm > 1e-30 ? sqrt(fm) : 1.0;
     }
 
     // ---------------------------------------------------------------------------------------------
@@ -148,53 +156,61 @@ struct Chain {
         sc.w1y = e.s * w1;
         sc.Rw2 = cc.Rw2;
         sc.Rw1 = cc.Rw1;
-        sc.cw = cc.cw;
 #pragma unroll
         for (int i = 0; i < NC; ++i) {
             sc.k[i] = cc.k[i];
             sc.kwc[i] = cc.kwc[i];
             sc.Rc2[i] = cc.Rc2[i];
             sc.Rc1[i] = cc.Rc1[i];
-            sc.cc[i] = cc.cc[i];
             sc.offc[i] = cc.offc0[i] - offw;                           // matrix.py:166
         }
         sc.kmt = cc.kmt;
         sc.kwmt = cc.kwmt;
         sc.Rm1W = cc.Rm1 + (w1 * w1) * g_mt;                           // matrix.py:210, 283
-        sc.cm = cc.cm;
     }
 
-    static __device__ __forceinline__ R coef_norm(const StepCoef<NC, D>& s) {
-        R sk = R(0);
+    // sqrt(a^2 + b^2) <= max + (sqrt(2) - 1) min, within 8.3%
+    static __device__ __forceinline__ R hyp(R a, R b) { return fmax(a, b) + R(0.41421357) * fmin(a, b); }
+
+    // An upper bound of ||D^-1 A D|| in the norm max_b ||v_b||_2 / d_b over blocks b = (x, y) pairs and
+    // z entries, with d = sqrt(f) per pool. The similarity balances the exchange terms (detailed
+    // balance: k f one way, k the other, so k sqrt(f) both ways) and each precession-relaxation block
+    // counts sqrt(R^2 + w^2) instead of R + w. Being an induced norm, it bounds ||X^k|| and so the
+    // Taylor tail; the truncation error of water's entries stays below tol times max(|M_w|,
+    // |M_c| / sqrt(f_c), 1).
+    static __device__ __forceinline__ R coef_norm(const StepCoef<NC, D>& s, const ChainConst<NC, D>& cc) {
+        // the constant column C enters through the augmented row: |C_i| / d_i
+        const R w1 = hyp(fabs(s.w1x.v), fabs(s.w1y.v));
+        R ex = R(0);
 #pragma unroll
-        for (int i = 0; i < NC; ++i) sk += fabs(s.k[i].v);
-        const R ax = fabs(s.w1x.v), ay = fabs(s.w1y.v), ow = fabs(s.offw.v);
-        R m = fabs(s.Rw2.v) + ow + fmax(ax, ay) + sk;
-        m = fmax(m, ax + ay + fabs(s.Rw1.v) + sk + fabs(s.kmt.v) + fabs(s.cw.v));
+        for (int i = 0; i < NC; ++i) ex += fabs(s.k[i].v) * R(cc.sf[i]);
+        R m = hyp(fabs(s.Rw2.v), fabs(s.offw.v)) + w1 + ex;
+        m = fmax(m, fabs(s.Rw1.v) + w1 + ex + fabs(s.kmt.v) * R(cc.sfm) + fabs(R(cc.cw.v)));
 #pragma unroll
         for (int i = 0; i < NC; ++i) {
-            const R b = fabs(s.kwc[i].v);
-            m = fmax(m, fabs(s.Rc2[i].v) + fabs(s.offc[i].v) + fmax(ax, ay) + b);
-            m = fmax(m, ax + ay + fabs(s.Rc1[i].v) + b + fabs(s.cc[i].v));
+            const R b = fabs(s.k[i].v) * R(cc.sf[i]);
+            m = fmax(m, hyp(fabs(s.Rc2[i].v), fabs(s.offc[i].v)) + w1 + b);
+            m = fmax(m, fabs(s.Rc1[i].v) + w1 + b + fabs(R(cc.cc[i].v)) / R(cc.sf[i]));
         }
-        m = fmax(m, fabs(s.Rm1W.v) + fabs(s.kwmt.v) + fabs(s.cm.v));
+        m = fmax(m, fabs(s.Rm1W.v) + fabs(s.kmt.v) * R(cc.sfm) + fabs(R(cc.cm.v)) / R(cc.sfm));
         return m;
     }
 
     static __device__ __forceinline__ void scale_coef(StepCoef<NC, D>& s, R h) {
-        s.Rw2 = h * s.Rw2; s.Rw1 = h * s.Rw1; s.cw = h * s.cw;
+        s.Rw2 = h * s.Rw2; s.Rw1 = h * s.Rw1;
 #pragma unroll
         for (int i = 0; i < NC; ++i) {
             s.k[i] = h * s.k[i]; s.kwc[i] = h * s.kwc[i]; s.Rc2[i] = h * s.Rc2[i];
-            s.Rc1[i] = h * s.Rc1[i]; s.cc[i] = h * s.cc[i]; s.offc[i] = h * s.offc[i];
+            s.Rc1[i] = h * s.Rc1[i]; s.offc[i] = h * s.offc[i];
         }
         s.offw = h * s.offw; s.w1x = h * s.w1x; s.w1y = h * s.w1y;
-        s.kmt = h * s.kmt; s.kwmt = h * s.kwmt; s.Rm1W = h * s.Rm1W; s.cm = h * s.cm;
+        s.kmt = h * s.kmt; s.kwmt = h * s.kwmt; s.Rm1W = h * s.Rm1W;
     }
 
     // y = X v (+ C h when WithC): the sparse Bloch-McConnell operator (matrix.py:238-293)
     template <bool WithC>
-    static __device__ __forceinline__ void matvec(const StepCoef<NC, D>& s, const State<NC, D>& v, State<NC, D>& y) {
+    static __device__ __forceinline__ void matvec(const StepCoef<NC, D>& s, const State<NC, D>& v, State<NC, D>& y,
+                                                  const ChainConst<NC, D>* cst = nullptr, R h = R(0)) {
         // water rows: own terms and the pools' exchange terms in two partial sums (shorter dependency
         // chains), pool rows: four terms each
         D xw = dfma(s.offw, v.yw, -(s.Rw2 * v.xw));
@@ -204,9 +220,9 @@ struct Chain {
         D zw = dfma(s.w1y, v.xw, -(s.Rw1 * v.zw));
         zw = zw - s.w1x * v.yw;
         D zm = dfma(s.kwmt, v.zw, -(s.Rm1W * v.zm));
-        if constexpr (WithC) {
-            zw = zw + s.cw;
-            zm = zm + s.cm;
+        if constexpr (WithC) {                     // the constant column C h, rebuilt here: it is needed
+            zw = dfma(cst->cw, dconst<R, NT>(h), zw);   // by the first term of a sub-step only
+            zm = dfma(cst->cm, dconst<R, NT>(h), zm);
         }
         D px = dconst<R, NT>(R(0)), py = px, pz = s.kmt * v.zm;
 #pragma unroll
@@ -223,7 +239,7 @@ struct Chain {
             D zc = dfma(s.kwc[i], v.zw, -(s.Rc1[i] * v.zc[i]));
             zc = dfma(s.w1y, v.xc[i], zc);
             zc = zc - s.w1x * v.yc[i];
-            if constexpr (WithC) zc = zc + s.cc[i];
+            if constexpr (WithC) zc = dfma(cst->cc[i], dconst<R, NT>(h), zc);
             y.xc[i] = xc;
             y.yc[i] = yc;
             y.zc[i] = zc;
@@ -266,11 +282,12 @@ struct Chain {
     // chain's result never depends on which chains share its warp.
     static __device__ __forceinline__ void taylor_apply(const StepCoef<NC, D>& s, int ns_w, int m_w, int ns_own,
                                                         int m_own, State<NC, D>& M,
-                                                        const double* __restrict__ inv_fact) {
+                                                        const double* __restrict__ inv_fact,
+                                                        const ChainConst<NC, D>& cst, R h) {
 #pragma unroll 1
         for (int j = 0; j < ns_w; ++j) {
             State<NC, D> term, acc = M;
-            matvec<true>(s, M, term);
+            matvec<true>(s, M, term, &cst, h);
             axpy_state(acc, term);
 #pragma unroll 1
             for (int k = 2; k <= m_w; ++k) {

@@ -6,7 +6,7 @@
 // exp([A C; 0 0] dt) [M; 1] is applied as a truncated Taylor series of matrix-vector products
 // with that operator (the action of the exponential, Al-Mohy & Higham, SIAM J. Sci. Comput. 33,
 // 2011), scaled into s sub-steps. Events whose exponential has a large norm (long delays, long CW
-// blocks) take a dense scaling-and-squaring path in bmc_dense.cuh instead.
+// blocks) take a dense scaling-and-squaring path (bmc_kernels.cuh, Dense) instead.
 //
 // Forward-mode tangents ride along as dual numbers `Dn<R, NT>`: every coefficient and every state
 // entry carries NT directional derivatives, so the tangent of Z is the exact derivative of the
@@ -186,16 +186,20 @@ struct ChainConst {
     S w0sl;                         // larmor * 1e-6: the super-Lorentzian bridge half width
     int ls;                         // 0 none, 1 Lorentzian, 2 super-Lorentzian
     bool mt_on;                     // f_mt > 1e-9 (matrix.py:203-213)
+    // balancing scales d = sqrt(f) of each CEST pool and of MT (1 where f is 0), for the norm only
+    double sf[NC > 0 ? NC : 1];
+    double sfm;
 };
 
 // the coefficients of one event, scaled by the sub-step h
+// (the constant column C is not here: it is rebuilt from ChainConst where the first term needs it)
 template <int NC, typename S>
 struct StepCoef {
-    S Rw2, Rw1, cw;
+    S Rw2, Rw1;
     S k[NC > 0 ? NC : 1], kwc[NC > 0 ? NC : 1], Rc2[NC > 0 ? NC : 1], Rc1[NC > 0 ? NC : 1];
-    S cc[NC > 0 ? NC : 1], offc[NC > 0 ? NC : 1];
+    S offc[NC > 0 ? NC : 1];
     S offw, w1x, w1y;
-    S kmt, kwmt, Rm1W, cm;
+    S kmt, kwmt, Rm1W;
 };
 
 template <int NC, typename V>

@@ -27,14 +27,29 @@ struct DenseSmem {
     using D = Dn<R, NT>;
     static constexpr int NA = Layout<NC>::NA;
     StepCoef<NC, D> coef;           // the owner chain's coefficients, scaled by dt / 2^s
+    D cw, cm, cc[NC > 0 ? NC : 1];  // ... and its constant column C, likewise scaled
     D mat[NA * NA];                 // column-major: column j at [j * NA]
     D vec[NA];                      // the owner's [M; 1]
     D out[NA];
     int s;
 };
 
+template <typename RD, typename RS, int NT>
+__device__ __forceinline__ Dn<RD, NT> cvt_dn(const Dn<RS, NT>& a) {
+    Dn<RD, NT> r;
+    r.v = RD(a.v);
+    if constexpr (NT > 0) {
+#pragma unroll
+        for (int t = 0; t < NT; ++t) r.d[t] = RD(a.d[t]);
+    }
+    return r;
+}
+
 template <int NC, typename R, int NT>
 struct Dense {
+    template <typename RS>
+    static __device__ __forceinline__ Dn<R, NT> cvt(const Dn<RS, NT>& a) { return cvt_dn<R, RS, NT>(a); }
+
     using D = Dn<R, NT>;
     using C = Chain<NC, R, NT>;
     using L = Layout<NC>;
@@ -43,14 +58,14 @@ struct Dense {
     using SM = DenseSmem<NC, R, NT>;
 
     // y = X_A v + C * caug: one column of X times a column of the matrix being built
-    static __device__ __forceinline__ void matvec_aug(const StepCoef<NC, D>& s, const State<NC, D>& v, R caug,
+    static __device__ __forceinline__ void matvec_aug(const SM* sm, const State<NC, D>& v, R caug,
                                                       State<NC, D>& y) {
-        C::template matvec<false>(s, v, y);
+        C::template matvec<false>(sm->coef, v, y);
         if (caug != R(0)) {
-            y.zw = y.zw + caug * s.cw;
-            y.zm = y.zm + caug * s.cm;
+            y.zw = y.zw + caug * sm->cw;
+            y.zm = y.zm + caug * sm->cm;
 #pragma unroll
-            for (int i = 0; i < NC; ++i) y.zc[i] = y.zc[i] + caug * s.cc[i];
+            for (int i = 0; i < NC; ++i) y.zc[i] = y.zc[i] + caug * sm->cc[i];
         }
     }
 
@@ -64,7 +79,9 @@ struct Dense {
             if (q == j) C::at(col, q) = dconst<R, NT>(R(1));
     }
 
-    static __device__ __noinline__ void event(SM* sm, int lane, bool evolve, const StepCoef<NC, D>& sc, R dt, R nu,
+    template <typename CC>
+    static __device__ __noinline__ void event(SM* sm, int lane, bool evolve, const StepCoef<NC, D>& sc, const CC& cst,
+                                              R dt, R nu,
                                  State<NC, D>& M, const TaylorTable& tt, int* status, bool count,
                                  unsigned long long& wh, unsigned long long& ws) {
         unsigned need = __ballot_sync(kFull, evolve);
@@ -79,8 +96,13 @@ struct Dense {
                     atomicOr(status, 2);
                 }
                 StepCoef<NC, D> scs = sc;
-                C::scale_coef(scs, R(ldexp(double(dt), -s)));
+                const R h = R(ldexp(double(dt), -s));
+                C::scale_coef(scs, h);
                 sm->coef = scs;
+                sm->cw = dconst<R, NT>(h) * cvt(cst.cw);
+                sm->cm = dconst<R, NT>(h) * cvt(cst.cm);
+#pragma unroll
+                for (int i = 0; i < NC; ++i) sm->cc[i] = dconst<R, NT>(h) * cvt(cst.cc[i]);
                 sm->s = s;
                 if (count) {
                     wh += (unsigned long long)NA * tt.dense_m;
@@ -99,7 +121,7 @@ struct Dense {
             if (lane < NA) {
                 for (int k = tt.dense_m; k >= 1; --k) {
                     State<NC, D> y;
-                    matvec_aug(sm->coef, col, caug, y);
+                    matvec_aug(sm, col, caug, y);
                     C::scal_state(y, R(tt.inv_k[k]));
                     State<NC, D> e;
                     unit(e, lane);
@@ -195,6 +217,7 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
     long long ci = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = ci < nch;
     if (!valid) ci = nch - 1;
+    if (a.order) ci = a.order[ci];                     // chains sorted by estimated cost (see cost_kernel)
     const int v = (int)(ci / a.n_off), o = (int)(ci % a.n_off);
     const bool act = valid && (a.active == nullptr || a.active[v] != 0);
     if (__all_sync(kFull, !act)) return;
@@ -236,7 +259,7 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
                 }
                 StepCoef<NC, D> sc;
                 C::event_coef(cc, rec, g, sc);
-                R nu = evolve ? rec.dt * C::coef_norm(sc) : R(0);
+                R nu = evolve ? rec.dt * C::coef_norm(sc, cc) : R(0);
                 if (!(nu < R(INFINITY))) {                          // NaN or inf: flag, let NaN propagate
                     if (evolve) atomicOr(a.status, 1);
                     nu = R(0);
@@ -246,14 +269,14 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
                 const bool dense_own = evolve && nu > R(tt.dense_switch);
                 if (__any_sync(kFull, dense_own)) {
                     if constexpr (std::is_same<R, RD>::value) {
-                        Dense<NC, R, NT>::event(dsm, lane, dense_own, sc, rec.dt, nu, M, tt, a.status, count, wk1, wk2);
+                        Dense<NC, R, NT>::event(dsm, lane, dense_own, sc, cc, rec.dt, nu, M, tt, a.status, count, wk1, wk2);
                     } else {
                         StepCoef<NC, Dn<RD, NT>> scd;
                         State<NC, Dn<RD, NT>> Md;
                         convert_flat<R, RD, NT>(sc, scd);
                         convert_flat<R, RD, NT>(M, Md);
-                        Dense<NC, RD, NT>::event(dsm, lane, dense_own, scd, RD(rec.dt), RD(nu), Md, tt, a.status, count,
-                                                 wk1, wk2);
+                        Dense<NC, RD, NT>::event(dsm, lane, dense_own, scd, cc, RD(rec.dt), RD(nu), Md, tt, a.status,
+                                                 count, wk1, wk2);
                         convert_flat<RD, R, NT>(Md, M);
                     }
                 }
@@ -269,8 +292,9 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
                 const int ns_w = __reduce_max_sync(kFull, (unsigned)ns_own);
                 const int m_w = __reduce_max_sync(kFull, (unsigned)m_own);
                 if (ns_w > 0) {
-                    C::scale_coef(sc, tay ? rec.dt / R(ns_own) : R(0));
-                    C::taylor_apply(sc, ns_w, m_w, ns_own, m_own, M, tt.inv_fact);
+                    const R h = tay ? rec.dt / R(ns_own) : R(0);
+                    C::scale_coef(sc, h);
+                    C::taylor_apply(sc, ns_w, m_w, ns_own, m_own, M, tt.inv_fact, cc, h);
                     if (count && tay) wk0 += (unsigned long long)ns_own * m_own;
                     if (count) wk3 += (unsigned long long)ns_w * m_w;
                 }
@@ -317,6 +341,35 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
             if (lane == 0 && x) atomicAdd(a.work + q, x);
         }
     }
+}
+
+// ------------------------------------------------------------------------------------------------
+// cost estimate of every chain: the norm of its first RF event's generator (what sets its Taylor
+// order), so that chains of equal order can share a warp
+// ------------------------------------------------------------------------------------------------
+template <int NC, typename R>
+__global__ void __launch_bounds__(128) cost_kernel(const ChainArgs a, float* __restrict__ key,
+                                                   int* __restrict__ idx) {
+    using C = Chain<NC, R, 0>;
+    using D = Dn<R, 0>;
+    const long long nch = (long long)a.n_vox * a.n_off;
+    const long long ci = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ci >= nch) return;
+    const int v = (int)(ci / a.n_off), o = (int)(ci % a.n_off);
+    const EvRec<R>* __restrict__ ev = reinterpret_cast<const EvRec<R>*>(a.ev);
+    float cost = 0.f;
+    for (int e = 0; e < a.n_ev; ++e) {
+        const EvRec<R> rec = ev[(size_t)e * a.n_off + o];
+        if ((int)rec.type != EV_RF || !(rec.dt > R(1e-9))) continue;
+        ChainConst<NC, D> cc;
+        C::load_const(a, v, 0, cc);
+        StepCoef<NC, D> sc;
+        C::event_coef(cc, rec, dconst<R, 0>(R(0)), sc);
+        cost = float(rec.dt * C::coef_norm(sc, cc));
+        break;
+    }
+    key[ci] = cost;
+    idx[ci] = (int)ci;
 }
 
 // ------------------------------------------------------------------------------------------------

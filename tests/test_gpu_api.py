@@ -95,7 +95,7 @@ def test_fit_batch_recovers_k_and_f(amide_ladder):
 
 def test_fit_batch_matches_the_oracle_lm_step_for_step(amide_ladder):
     """Same start, same damping schedule, float64 on both sides: the device LM and the oracle LM
-    land on the same parameters (0.1% target; held to 1e-6)."""
+    land on the same parameters (0.1% target; held to 1e-5 on a noisy, ill-conditioned slow pool)."""
     from bmc_b200.fitting import FitSpec, FreeParam, fit_batch
     p, jp, base, events, M0, Z = amide_ladder
     spec = FitSpec([FreeParam("k", "cest_k", 0, scale=100.0, lo=5.0, hi=2000.0, x0=150.0),
@@ -109,7 +109,7 @@ def test_fit_batch_matches_the_oracle_lm_step_for_step(amide_ladder):
         op = O.Params(*[np.asarray(v)[i] for v in sub])
         x = O.fit_voxel(op, ev, M0[i], [O.Slot("cest_k", 0, 100.0), O.Slot("cest_f", 0, 0.001)], zn[i],
                         [150.0, 0.0005], [5.0, 1e-5], [2000.0, 0.01], n_iter=12)
-        np.testing.assert_allclose(X[i], x, rtol=1e-6)
+        np.testing.assert_allclose(X[i], x, rtol=1e-5)     # target 1e-3; rounding differs (Taylor vs Pade)
 
 
 # ---- joint fits (tests/test_joint.py) -----------------------------------------------------------
@@ -178,10 +178,12 @@ def test_joint_jacobian_is_the_derivative(joint3):
         x = d["x0"] + 0.02 * np.linspace(-1.0, 1.0, d["x0"].size)
         J = d["jac"](x)
         Ja = np.empty_like(J)
-        for j in range(x.size):
-            h = 1e-6 * max(1.0, abs(x[j]))
+        for j in range(x.size):                    # Richardson-extrapolated central differences
+            h = 1e-4 * max(1.0, abs(x[j]))
             e = np.zeros(x.size); e[j] = h
-            Ja[:, j] = (d["resid"](x + e) - d["resid"](x - e)) / (2 * h)
+            d1 = (d["resid"](x + e) - d["resid"](x - e)) / (2 * h)
+            d2 = (d["resid"](x + e / 2) - d["resid"](x - e / 2)) / h
+            Ja[:, j] = (4 * d2 - d1) / 3
         rel = np.linalg.norm(J - Ja, axis=0) / np.maximum(np.linalg.norm(Ja, axis=0), 1e-30)
         assert rel.max() < 1e-4, f"{[s.name for s in slots]}: {rel}"      # the reference's own bound
 
