@@ -24,7 +24,7 @@ SLOT_SPREAD_SIGMA, SLOT_M_START = -2, -3
 
 EXPORTS = ("bmc_abi_version", "bmc_version", "bmc_last_error", "bmc_release", "bmc_simulate",
            "bmc_simulate_jvp", "bmc_simulate_trajectory", "bmc_lm_fit", "bmc_normal_blocks",
-           "bmc_simulate_counted", "bmc_probe_fma_peak")
+           "bmc_simulate_counted", "bmc_probe_fma_peak", "bmc_simulate_noalloc")
 
 
 class Problem(C.Structure):
@@ -90,6 +90,8 @@ def lib():
         L.bmc_simulate_counted.restype = C.c_int
         L.bmc_probe_fma_peak.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double), vp]
         L.bmc_probe_fma_peak.restype = C.c_int
+        L.bmc_simulate_noalloc.argtypes = [C.POINTER(Problem), vp, C.POINTER(Events), vp, C.POINTER(Spread), vp, vp]
+        L.bmc_simulate_noalloc.restype = C.c_int
         _lib = L
     return _lib
 

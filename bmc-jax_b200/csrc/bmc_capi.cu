@@ -580,3 +580,114 @@ bmc_status bmc_probe_fma_peak(int32_t precision, int32_t blocks, int32_t iters, 
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------------
+// bmc_simulate_noalloc: the forward model with no device allocation at all
+// ------------------------------------------------------------------------------------------------
+// Some callers cannot let a library call cudaMalloc: a handler running inside JAX/XLA (JAX reserves
+// most of the GPU's memory for its own allocator up front, so a cudaMalloc there can fail, and memory
+// taken behind XLA's back is not accounted for), code running under another framework's caching
+// allocator with a fixed memory budget, and latency-bound pipelines, for which cudaMalloc/cudaFree
+// are unbounded-latency calls that synchronise the device. For them this entry point takes its only
+// scratch -- the preprocessed event records and a status word -- from one static device array,
+// g_noalloc_scratch, of kNoAllocScratchBytes on every GPU that loads the library (held until the
+// process exits). The chains run in launch order (no cost sort, which would need more scratch); the
+// results are bit-identical to bmc_simulate's, whose chains each choose their own Taylor order.
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;     // 32 MiB per GPU
+constexpr size_t kNoAllocStatusBytes = 256;
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};               // device address of the array, per device
+bool g_noalloc_tables[kNoAllocMaxDevices] = {};
+
+// Once per device, with that device current: the device address of the static array (in host code
+// its name is only a host-side stand-in) and the Taylor tables. Runs inside the first call on a
+// device, which should therefore come before any stream capture.
+bmc_status noalloc_setup(int precision, void** scratch, const TaylorTable** tt) {
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices)
+        return fail(BMC_ERR_UNSUPPORTED, "bmc_simulate_noalloc: device %d above %d", dev, kNoAllocMaxDevices - 1);
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_tables[dev]) {
+        TaylorTable h[2] = {make_table(1e-13, 30, 0.5, 100.0), make_table(std::ldexp(1.0, -24), 16, 0.5, 100.0)};
+        CUDA_TRY(cudaMemcpyToSymbol(g_tables, h, sizeof(h)));
+        g_noalloc_tables[dev] = true;
+    }
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(BMC_ERR_CUDA, "bmc_simulate_noalloc: cudaGetSymbolAddress of the static scratch: %s",
+                        cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = p;
+    }
+    TaylorTable* t = nullptr;
+    CUDA_TRY(cudaGetSymbolAddress((void**)&t, g_tables));
+    *tt = t + (precision == BMC_F32 ? 1 : 0);
+    *scratch = g_noalloc_ptr[dev];
+    return BMC_OK;
+}
+
+template <int NC>
+struct NoAlloc {
+    template <typename R>
+    static bmc_status run(const bmc_problem* pr, const double* params, const bmc_events* ev, const double* m0,
+                          const bmc_spread* sp, double* out, void* scratch, const TaylorTable* tt, cudaStream_t st) {
+        ChainArgs a{};
+        a.n_vox = pr->n_voxels; a.n_off = pr->n_offsets; a.n_ev = pr->n_events; a.n_fields = Layout<NC>::NF;
+        a.mz = pr->mz_loc; a.reset_after_adc = pr->reset_after_adc;
+        bmc_status s = fill_spread(a, sp);
+        if (s != BMC_OK) return s;
+        a.params = params; a.m0 = m0; a.out = out;
+        a.status = static_cast<int*>(scratch);
+        CUDA_TRY(cudaMemsetAsync(a.status, 0, sizeof(int), st));          // must start at zero each call
+        EvRec<R>* rec = reinterpret_cast<EvRec<R>*>(static_cast<char*>(scratch) + kNoAllocStatusBytes);
+        if ((s = prep_events<R>(pr, ev, rec, st)) != BMC_OK) return s;   // overwrites the previous call's
+        a.ev = rec;
+        return launch_chain<NC, R, 0>(a, tt, st);
+    }
+
+    static bmc_status simulate(const bmc_problem* pr, const double* params, const bmc_events* ev, const double* m0,
+                               const bmc_spread* sp, double* out, void* scratch, const TaylorTable* tt,
+                               cudaStream_t st) {
+        return pr->precision == BMC_F32 ? run<float>(pr, params, ev, m0, sp, out, scratch, tt, st)
+                                        : run<double>(pr, params, ev, m0, sp, out, scratch, tt, st);
+    }
+};
+
+}  // namespace
+
+extern "C" bmc_status bmc_simulate_noalloc(const bmc_problem* prob, const double* d_params, const bmc_events* ev,
+                                           const double* d_m0, const bmc_spread* spread, double* d_out,
+                                           void* stream) {
+    bmc_status s = check_problem(prob, d_params, ev, d_m0);
+    if (s != BMC_OK) return s;
+    if (!d_out) return fail(BMC_ERR_INVALID, "null output");
+    const size_t rec_bytes = prob->precision == BMC_F32 ? sizeof(EvRec<float>) : sizeof(EvRec<double>);
+    const size_t nrec = (size_t)prob->n_offsets * (size_t)prob->n_events;
+    const size_t cap = (kNoAllocScratchBytes - kNoAllocStatusBytes) / rec_bytes;
+    if (nrec > cap)
+        return fail(BMC_ERR_INVALID,
+                    "bmc_simulate_noalloc: the event table (%d offsets x %d events = %zu records of %zu bytes) "
+                    "exceeds its static scratch of %zu bytes (at most %zu records); use bmc_simulate",
+                    prob->n_offsets, prob->n_events, nrec, rec_bytes, kNoAllocScratchBytes, cap);
+    void* scratch = nullptr;
+    const TaylorTable* tt = nullptr;
+    if ((s = noalloc_setup(prob->precision, &scratch, &tt)) != BMC_OK) return s;
+    const cudaStream_t st = (cudaStream_t)stream;
+    switch (prob->n_cest) {
+        case 0: return NoAlloc<0>::simulate(prob, d_params, ev, d_m0, spread, d_out, scratch, tt, st);
+        case 1: return NoAlloc<1>::simulate(prob, d_params, ev, d_m0, spread, d_out, scratch, tt, st);
+        case 2: return NoAlloc<2>::simulate(prob, d_params, ev, d_m0, spread, d_out, scratch, tt, st);
+        case 3: return NoAlloc<3>::simulate(prob, d_params, ev, d_m0, spread, d_out, scratch, tt, st);
+        case 4: return NoAlloc<4>::simulate(prob, d_params, ev, d_m0, spread, d_out, scratch, tt, st);
+        case 5: return NoAlloc<5>::simulate(prob, d_params, ev, d_m0, spread, d_out, scratch, tt, st);
+        default: return fail(BMC_ERR_UNSUPPORTED, "n_cest %d", prob->n_cest);
+    }
+}

@@ -174,6 +174,22 @@ bmc_status bmc_normal_blocks(int32_t n_voxels, int32_t n_points, int32_t n_tange
                              double* d_c, void* stream);
 
 /*
+ * bmc_simulate without any device allocation. No counterpart in the reference: an addition for
+ * callers that cannot let a library call cudaMalloc -- a handler inside JAX/XLA (JAX reserves most of
+ * the GPU's memory for its own allocator), code under another framework's fixed memory budget, or a
+ * latency-bound pipeline (cudaMalloc/cudaFree synchronise the device). Same arguments and results as
+ * bmc_simulate (bit-identical Z). Its only scratch, the preprocessed event records and a status word,
+ * lives in one static device array of 32 MiB per GPU that loads the library, held until exit, so
+ * n_offsets x n_events may be at most 699,045 records in float64 (1,048,568 in float32); larger tables
+ * are rejected with BMC_ERR_INVALID and a message. The first call on a device takes the array's
+ * device address and uploads the Taylor tables (issue it before any stream capture). Every call reuses
+ * the same array and overwrites the previous call's records: calls that overlap on the GPU (other
+ * streams, other host threads) race and must be serialised by the caller.
+ */
+bmc_status bmc_simulate_noalloc(const bmc_problem* prob, const double* d_params, const bmc_events* ev,
+                                const double* d_m0, const bmc_spread* spread, double* d_out, void* stream);
+
+/*
  * Diagnostics (no counterpart in the reference: measurement support for the benchmark).
  * bmc_simulate_counted: bmc_simulate that also adds the work it executed to d_work[4] (device,
  *   zeroed by the caller): [0] Taylor sub-step terms each chain needed (one sparse operator product
