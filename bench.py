@@ -309,6 +309,186 @@ def run_ours(args, rank, world, local_rank):
     return line
 
 
+def quesp_ladder(n_ppm=61, b1s=(0.5, 1.0, 2.0, 4.0), tsat=2.0, b0=3.0):
+    """The configuration-1 sequence: one CW block per offset then the ADC, four rungs stacked."""
+    ppm = np.linspace(-6.0, 6.0, n_ppm)
+    rows = []
+    for b1 in b1s:
+        amp = b1 * GAMMA / (2 * np.pi)
+        fr = ppm * 42.5764 * b0
+        rows.append((np.tile(np.int32([1, 3]), (n_ppm, 1)), np.tile([tsat, 0.0], (n_ppm, 1)),
+                     np.tile([amp, 0.0], (n_ppm, 1)), np.zeros((n_ppm, 2)),
+                     np.stack([fr, np.zeros(n_ppm)], axis=1), np.tile(np.int32([-1, 0]), (n_ppm, 1))))
+    return tuple(np.ascontiguousarray(np.concatenate([r[i] for r in rows])) for i in range(6))
+
+
+def run_fit(args, rank, world, local_rank):
+    """Fitted voxels/s: (k, f) of an amide pool (configuration 1's model at 3 T) from (300, 5e-4),
+    30 LM iterations on the device, noise-free data; a voxel counts as fitted when both parameters are
+    within 1% of the truth that made its data."""
+    import torch
+    import ctypes as C
+    from bmc_b200 import _lib
+    from bmc_b200.simulation import DeviceEvents, problem
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    n = args.voxels
+    rng = np.random.default_rng(rank_seed(rank))
+    k_true = rng.uniform(20.0, 1000.0, n)
+    f_true = rng.uniform(3e-4, 3e-3, n)
+    rows = [np.full(n, 1 / 1.3), np.full(n, 1 / 0.05), np.ones(n), k_true, f_true, np.full(n, 3.5),
+            np.full(n, 1 / 1.3), np.full(n, 1 / 0.1), np.zeros(n), np.zeros(n), np.zeros(n), np.zeros(n),
+            np.ones(n), np.zeros(n), np.full(n, B0), np.full(n, GAMMA), np.zeros(n), np.ones(n)]
+    P = np.ascontiguousarray(np.stack(rows))
+    M0 = np.zeros((n, 7)); M0[:, 4] = 1.0; M0[:, 5] = f_true
+    ev = quesp_ladder()
+    n_off, n_ev = ev[0].shape
+    dev_ev = DeviceEvents.from_tensors(*[torch.as_tensor(a).to(dev) for a in ev])
+    dP, dM = torch.as_tensor(P).to(dev), torch.as_tensor(M0).to(dev)
+    L = _lib.lib()
+    sh = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    pr = problem(n, n_off, n_ev, 1, 4, _lib.F64)
+    z = torch.empty((n, n_off), dtype=torch.float64, device=dev)
+    _lib.check(L.bmc_simulate(pr, C.c_void_p(dP.data_ptr()), dev_ev.struct, C.c_void_p(dM.data_ptr()), None,
+                              C.c_void_p(z.data_ptr()), sh))
+    spec = _lib.FitSpecC()
+    spec.n_params, spec.n_iter, spec.lam0 = 2, 30, 1e-2
+    for p, (row, sc, lo, hi) in enumerate([(3, 100.0, 5.0, 5000.0), (4, 1e-3, 1e-6, 0.05)]):
+        spec.field_row[p], spec.mode[p], spec.scale[p] = row, 0, sc
+        spec.lo[p], spec.hi[p] = lo / sc, hi / sc
+    x0 = torch.tensor(np.tile([3.0, 0.5], (n, 1)), dtype=torch.float64, device=dev)
+    xo = torch.empty((n, 2), dtype=torch.float64, device=dev)
+
+    def step():
+        _lib.check(L.bmc_lm_fit(pr, C.c_void_p(dP.data_ptr()), dev_ev.struct, C.c_void_p(dM.data_ptr()), None, spec,
+                                C.c_void_p(z.data_ptr()), C.c_void_p(x0.data_ptr()), C.c_void_p(xo.data_ptr()),
+                                None, None, sh))
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    times = []
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step()
+        e1.record()
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = max_over_ranks(float(np.mean(times)), dev)
+    x = xo.cpu().numpy() * np.array([100.0, 1e-3])
+    ok = (np.abs(x[:, 0] / k_true - 1) <= 0.01) & (np.abs(x[:, 1] / f_true - 1) <= 0.01)
+    return {"metric": "fitted voxels/s at <=1% param err (plain LM, device)", "value": world * n * ok.mean() / (ms * 1e-3),
+            "unit": "voxels/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded), noise-free",
+            "config": {"workload": f"LM fit of (k, f), amide pool at 3 T, QUESP ladder 4 x 61 CW offsets (2 s), "
+                                   f"{n} voxels per GPU, 30 iterations from (300, 5e-4)",
+                       "fraction_within_1pct": float(ok.mean()), "voxels_per_gpu": n}}
+
+
+PHANTOM = ROOT / "tests" / "golden" / "phantom"
+PUBLISHED_S = {"phantom08": 15 * 60.0, "phantom09": 15 * 60.0, "phantom10": 2 * 3600.0}   # 1x RTX 3070
+
+
+def phantom_data(tubes=None):
+    """The shipped phantom measurement (tests/golden/phantom), optionally only the tubes with a pool."""
+    with np.load(PHANTOM / "phantom_7tubes.npz", allow_pickle=True) as d:
+        data = {k: d[k] for k in d.files}
+    if tubes == "pool":
+        idx = np.flatnonzero(np.isfinite(data["vial_dw"]))
+        per = ("Z_quesp", "Z_quest", "vial_names", "vial_dw", "R1", "b0_hz", "rel_b1", "noise_quesp", "noise_quest")
+        data = {k: (v[idx] if k in per else v) for k, v in data.items()}
+    return data
+
+
+def phantom_params(d, pool_t2_s=0.010):
+    """Every tube as one batched SimParams: measured water R1, B0 and B1 per tube, PBS water R2 for all,
+    the CEST pool at its shift with T2 pool_t2_s (k and f are placeholders the fit replaces)."""
+    from bmc_b200.simulation import SimParams
+    n = len(d["vial_names"])
+    one = np.ones(n)
+    pool = np.isfinite(d["vial_dw"])
+    b0 = float(d["b0_T"])
+    return SimParams(water_r1=d["R1"].astype(float), water_r2=float(d["water_r2"]) * one, water_f=one,
+                     cest_k=np.where(pool, 900.0, 0.0)[:, None], cest_f=np.where(pool, 0.008, 0.0)[:, None],
+                     cest_dw=np.where(pool, d["vial_dw"], 0.0)[:, None].astype(float), cest_r1=one[:, None],
+                     cest_r2=(one / pool_t2_s)[:, None], mt_k=0 * one, mt_f=0 * one, mt_dw=0 * one,
+                     mt_r1=0 * one, mt_r2=one, mt_lineshape=np.zeros(n, np.int32), b0=b0 * one,
+                     gamma=267.5153 * one, b0_inhom=d["b0_hz"] / (42.5764 * b0), rel_b1=d["rel_b1"].astype(float))
+
+
+def phantom_events(stem, keep):
+    """One rung's converted sequence, the -300 ppm reference row dropped, offsets masked by keep."""
+    from bmc_b200.simulation import SimEvent
+    with np.load(PHANTOM / f"{stem}_events.npz") as d:
+        ev = SimEvent(*[np.asarray(d[f])[1:] for f in SimEvent._fields])
+    return SimEvent(*[a[keep] for a in ev])
+
+
+def run_phantom(args):
+    """Tutorials 08 (QUESP fit), 09 (QUEST fit) and 10 (joint fit: shared water R2 factor, M_start and a
+    15-node B0 spread) of the reference on the shipped phantom data, through bmc_b200's public API; the
+    wall time of the fit call, host<->device traffic included, against the published RTX 3070 runtime."""
+    import torch
+    from dataclasses import replace
+    from bmc_b200.fitting import Experiment, FitSpec, FreeParam, fit, fit_joint
+    from bmc_b200.simulation import initial_state, SimParams, B0Spread
+    torch.cuda.init()
+    w = args.workload
+
+    def ladder_for(d, rungs, kind):
+        p = phantom_params(d)
+        n = len(d["vial_names"])
+        m0 = np.stack([initial_state(SimParams(*[np.asarray(v)[i] for v in p]), float(d["m_start"])) for i in range(n)])
+        keep = np.abs(d["ppm"]) >= 1.0
+        stems = ([f"quesp_sim_b1_{('%g' % b).replace('.', 'p')}uT" for b in rungs] if kind == "quesp" else
+                 [f"quest_sim_tsat_{('%g' % t).replace('.', 'p')}s" for t in rungs])
+        lad = Experiment.stack([Experiment(p, phantom_events(s, keep), m0, 4) for s in stems])
+        Z = d["Z_" + kind][:, :, keep].reshape(n, -1)
+        return lad, Z, int(keep.sum())
+
+    K = FreeParam("k", "cest_k", 0, scale=1000.0, lo=5.0, hi=2000.0, x0=300.0)
+    F = FreeParam("f", "cest_f", 0, scale=0.01, lo=1e-5, hi=0.03, x0=0.008)
+    T2 = FreeParam("r2p", "cest_r2", 0, scale=100.0, lo=10.0, hi=1000.0, x0=100.0)
+    d6 = phantom_data("pool")
+    kind = "quest" if w == "phantom09" else "quesp"
+    rungs = d6["tsat_s"] if kind == "quest" else d6["b1_levels_uT"]
+    lad6, Z6, n_per = ladder_for(d6, rungs, kind)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain = fit(lad6, FitSpec([K, F, T2]), Z6, n_iter=60, n_per_block=n_per)
+    t_plain = time.perf_counter() - t0
+    out = {"fit_s": t_plain, "tubes": [str(s) for s in d6["vial_names"]], "k": plain["k"].tolist(),
+           "f": plain["f"].tolist(), "t2_pool_ms": (1e3 / plain["r2p"]).tolist(),
+           "rms_over_noise": (plain.rms / d6["noise_" + kind]).tolist(),
+           "points": int(Z6.shape[1]), "events": lad6.n_events}
+    value = t_plain
+    if w == "phantom10":
+        d7 = phantom_data()
+        pool = tuple(int(i) for i in np.flatnonzero(np.isfinite(d7["vial_dw"])))
+        Kp, Fp, T2p = (replace(s, samples=pool) for s in (K, F, T2))
+        R2F = FreeParam("r2w", "water_r2", None, scale=1.0, lo=0.5, hi=2.0, x0=1.0, scope="shared", mode="factor")
+        MS = FreeParam("m_start", "m_start", None, scale=1.0, lo=0.2, hi=1.0, x0=float(d7["m_start"]), scope="shared")
+        SIG = FreeParam("sigma", "b0_spread", None, scale=10.0, lo=0.0, hi=8.0, x0=5.0, scope="shared")
+        spec = FitSpec([Kp, Fp, T2p, R2F, MS, SIG])
+        x0 = np.tile([s.x0 for s in spec.slots], (7, 1))
+        x0[list(pool), :3] = plain.x
+        lad7, Z7, _ = ladder_for(d7, d7["b1_levels_uT"], "quesp")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        joint = fit_joint(lad7, spec, Z7, n_iter=12, n_per_block=n_per, x0_phys=x0, spread=B0Spread(nodes=15))
+        t_joint = time.perf_counter() - t0
+        value = t_plain + t_joint
+        out.update(joint_s=t_joint, r2w=float(joint["r2w"][0]), m_start=float(joint["m_start"][0]),
+                   sigma_hz=float(joint["sigma"][0]), joint_cost=[float(joint.cost[0]), float(joint.cost[-1])])
+    pub = PUBLISHED_S[w]
+    return {"metric": f"wall time of the reference's tutorial {w[-2:]} fit (public API, end to end)", "value": value,
+            "unit": "s", "n_gpus": 1, "higher_is_better": False, "vs_baseline": value / pub,
+            "published_s": pub, "published_on": "1x RTX 3070 (examples/README.md)", "dtype": "f64",
+            "data": "the reference's shipped phantom measurement", "config": {"workload": w, **out}}
+
+
 def run_reference(args):
     nc = args.pools
     P, M0 = voxel_params(max(args.voxels, 1), nc, seed=1000)
@@ -337,6 +517,8 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["forward", "fit", "phantom08", "phantom09", "phantom10"],
+                    default="forward")
     ap.add_argument("--voxels", type=int, default=65536)
     ap.add_argument("--offsets", type=int, default=101)
     ap.add_argument("--pulses", type=int, default=20)
@@ -359,7 +541,11 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
-    line = run_ours(args, rank, world, local_rank)
+    if args.workload.startswith("phantom"):
+        if rank == 0:
+            print(json.dumps(run_phantom(args)), flush=True)
+        return
+    line = (run_fit if args.workload == "fit" else run_ours)(args, rank, world, local_rank)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

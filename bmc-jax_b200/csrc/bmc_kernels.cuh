@@ -22,8 +22,16 @@ __device__ __forceinline__ R warp_max(R x) {
 // Taylor action would need ~||X|| sub-steps. Instead the warp forms exp(X) by scaling and squaring:
 // exp(X / 2^s) by a degree-m Horner recurrence (each column by the sparse operator, in registers),
 // then s squarings through shared memory, then the matrix-vector product with [M; 1].
+// lanes per chain in the dense path: one column per lane, so a warp works on 32 / group chains at once
+template <int NC>
+struct DenseGroup {
+    static constexpr int NA = Layout<NC>::NA;
+    static constexpr int GS = NA <= 8 ? 8 : (NA <= 16 ? 16 : 32);
+    static constexpr int G = 32 / GS;
+};
+
 template <int NC, typename R, int NT>
-struct DenseSmem {
+struct DenseSlot {
     using D = Dn<R, NT>;
     static constexpr int NA = Layout<NC>::NA;
     StepCoef<NC, D> coef;           // the owner chain's coefficients, scaled by dt / 2^s
@@ -32,6 +40,11 @@ struct DenseSmem {
     D vec[NA];                      // the owner's [M; 1]
     D out[NA];
     int s;
+};
+
+template <int NC, typename R, int NT>
+struct DenseSmem {
+    DenseSlot<NC, R, NT> slot[DenseGroup<NC>::G];
 };
 
 template <typename RD, typename RS, int NT>
@@ -57,15 +70,19 @@ struct Dense {
     static constexpr int NA = L::NA;
     using SM = DenseSmem<NC, R, NT>;
 
+    using SL = DenseSlot<NC, R, NT>;
+    static constexpr int GS = DenseGroup<NC>::GS;
+    static constexpr int G = DenseGroup<NC>::G;
+
     // y = X_A v + C * caug: one column of X times a column of the matrix being built
-    static __device__ __forceinline__ void matvec_aug(const SM* sm, const State<NC, D>& v, R caug,
+    static __device__ __forceinline__ void matvec_aug(const SL* sl, const State<NC, D>& v, R caug,
                                                       State<NC, D>& y) {
-        C::template matvec<false>(sm->coef, v, y);
+        C::template matvec<false>(sl->coef, v, y);
         if (caug != R(0)) {
-            y.zw = y.zw + caug * sm->cw;
-            y.zm = y.zm + caug * sm->cm;
+            y.zw = y.zw + caug * sl->cw;
+            y.zm = y.zm + caug * sl->cm;
 #pragma unroll
-            for (int i = 0; i < NC; ++i) y.zc[i] = y.zc[i] + caug * sm->cc[i];
+            for (int i = 0; i < NC; ++i) y.zc[i] = y.zc[i] + caug * sl->cc[i];
         }
     }
 
@@ -79,16 +96,26 @@ struct Dense {
             if (q == j) C::at(col, q) = dconst<R, NT>(R(1));
     }
 
+    // Every lane whose `evolve` is set gets its state advanced by exp(X) [M; 1]. The warp takes up to
+    // G of those chains at a time: chain g of a round is done by lanes g GS .. g GS + NA - 1, lane
+    // g GS + j owning column j.
     template <typename CC>
     static __device__ __noinline__ void event(SM* sm, int lane, bool evolve, const StepCoef<NC, D>& sc, const CC& cst,
-                                              R dt, R nu,
-                                 State<NC, D>& M, const TaylorTable& tt, int* status, bool count,
-                                 unsigned long long& wh, unsigned long long& ws) {
+                                              R dt, R nu, State<NC, D>& M, const TaylorTable& tt, int* status,
+                                              bool count, unsigned long long& wh, unsigned long long& ws) {
+        const int grp = lane / GS, gl = lane % GS;
         unsigned need = __ballot_sync(kFull, evolve);
         while (need) {
-            const int c = __ffs(need) - 1;
-            need &= need - 1;
-            if (lane == c) {
+            int my_slot = -1, grp_owner = -1;
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+                const int c = need ? __ffs(need) - 1 : -1;
+                if (need) need &= need - 1;
+                if (c == lane) my_slot = g;
+                if (g == grp) grp_owner = c;
+            }
+            if (my_slot >= 0) {
+                SL* sl = &sm->slot[my_slot];
                 int s = 0;
                 if (nu > R(tt.dense_theta)) s = (int)ceil(log2(double(nu) / tt.dense_theta));
                 if (s > 200) {
@@ -98,77 +125,81 @@ struct Dense {
                 StepCoef<NC, D> scs = sc;
                 const R h = R(ldexp(double(dt), -s));
                 C::scale_coef(scs, h);
-                sm->coef = scs;
-                sm->cw = dconst<R, NT>(h) * cvt(cst.cw);
-                sm->cm = dconst<R, NT>(h) * cvt(cst.cm);
+                sl->coef = scs;
+                sl->cw = dconst<R, NT>(h) * cvt(cst.cw);
+                sl->cm = dconst<R, NT>(h) * cvt(cst.cm);
 #pragma unroll
-                for (int i = 0; i < NC; ++i) sm->cc[i] = dconst<R, NT>(h) * cvt(cst.cc[i]);
-                sm->s = s;
+                for (int i = 0; i < NC; ++i) sl->cc[i] = dconst<R, NT>(h) * cvt(cst.cc[i]);
+                sl->s = s;
                 if (count) {
                     wh += (unsigned long long)NA * tt.dense_m;
                     ws += (unsigned long long)s;
                 }
 #pragma unroll
-                for (int q = 0; q < N; ++q) sm->vec[q] = C::at(M, q);
-                sm->vec[N] = dconst<R, NT>(R(1));
+                for (int q = 0; q < N; ++q) sl->vec[q] = C::at(M, q);
+                sl->vec[N] = dconst<R, NT>(R(1));
             }
             __syncwarp();
-            const int s = sm->s;
+            SL* sl = &sm->slot[grp];
+            const bool work = grp_owner >= 0 && gl < NA;
+            const int s = grp_owner >= 0 ? sl->s : 0;
+            const int smax = (int)__reduce_max_sync(kFull, (unsigned)s);
             State<NC, D> col;
-            const R caug = (lane == N) ? R(1) : R(0);
-            // Horner: T = I + X T / k, k = m .. 1  (column `lane`)
-            unit(col, lane);
-            if (lane < NA) {
+            const R caug = (gl == N) ? R(1) : R(0);
+            // Horner: T = I + X T / k, k = m .. 1  (column gl)
+            unit(col, gl);
+            if (work) {
                 for (int k = tt.dense_m; k >= 1; --k) {
                     State<NC, D> y;
-                    matvec_aug(sm, col, caug, y);
+                    matvec_aug(sl, col, caug, y);
                     C::scal_state(y, R(tt.inv_k[k]));
                     State<NC, D> e;
-                    unit(e, lane);
+                    unit(e, gl);
                     C::axpy_state(e, y);
                     col = e;
                 }
             }
             // s squarings: column j of T T is sum_l T[:, l] T[l][j]
-            for (int q = 0; q < s; ++q) {
-                if (lane < NA) {
+            for (int q = 0; q < smax; ++q) {
+                const bool sq = work && q < s;
+                if (sq) {
 #pragma unroll
-                    for (int i = 0; i < N; ++i) sm->mat[lane * NA + i] = C::at(col, i);
-                    sm->mat[lane * NA + N] = dconst<R, NT>(caug);
+                    for (int i = 0; i < N; ++i) sl->mat[gl * NA + i] = C::at(col, i);
+                    sl->mat[gl * NA + N] = dconst<R, NT>(caug);
                 }
                 __syncwarp();
-                if (lane < NA) {
+                if (sq) {
                     State<NC, D> nc;
                     unit(nc, -1);
 #pragma unroll
                     for (int l = 0; l < N; ++l) {
                         const D w = C::at(col, l);
 #pragma unroll
-                        for (int i = 0; i < N; ++i) C::at(nc, i) = dfma(sm->mat[l * NA + i], w, C::at(nc, i));
+                        for (int i = 0; i < N; ++i) C::at(nc, i) = dfma(sl->mat[l * NA + i], w, C::at(nc, i));
                     }
                     if (caug != R(0)) {           // the augmented column also picks up T[:, aug]
 #pragma unroll
-                        for (int i = 0; i < N; ++i) C::at(nc, i) = C::at(nc, i) + sm->mat[N * NA + i];
+                        for (int i = 0; i < N; ++i) C::at(nc, i) = C::at(nc, i) + sl->mat[N * NA + i];
                     }
                     col = nc;
                 }
                 __syncwarp();
             }
             // M <- T [M; 1]
-            if (lane < NA) {
+            if (work) {
 #pragma unroll
-                for (int i = 0; i < N; ++i) sm->mat[lane * NA + i] = C::at(col, i);
+                for (int i = 0; i < N; ++i) sl->mat[gl * NA + i] = C::at(col, i);
             }
             __syncwarp();
-            if (lane < N) {
+            if (grp_owner >= 0 && gl < N) {
                 D acc = dconst<R, NT>(R(0));
-                for (int j = 0; j < NA; ++j) acc = dfma(sm->mat[j * NA + lane], sm->vec[j], acc);
-                sm->out[lane] = acc;
+                for (int j = 0; j < NA; ++j) acc = dfma(sl->mat[j * NA + gl], sl->vec[j], acc);
+                sl->out[gl] = acc;
             }
             __syncwarp();
-            if (lane == c) {
+            if (my_slot >= 0) {
 #pragma unroll
-                for (int q = 0; q < N; ++q) C::at(M, q) = sm->out[q];
+                for (int q = 0; q < N; ++q) C::at(M, q) = sm->slot[my_slot].out[q];
             }
             __syncwarp();
         }
