@@ -1,9 +1,19 @@
-"""Saturation sequences built in code (BMC-JAX sequences/saturation.py:17-84)."""
+"""Saturation sequences built in code (BMC-JAX sequences/saturation.py:17-84); the Pulseq converter
+(`events_from_seq`, `events_from_seq_batch`, `prep_rf_simulation`, module `pulseq`) is imported on
+first use, as in BMC-JAX sequences/__init__.py:11-15."""
 import numpy as np
 
 from .simulation import EventType, SimEvent
 
-__all__ = ["GAMMA_RAD_PER_S_UT", "GAMMA_HZ_PER_T", "hz_per_ppm", "cw_saturation"]
+__all__ = ["GAMMA_RAD_PER_S_UT", "GAMMA_HZ_PER_T", "hz_per_ppm", "cw_saturation", "events_from_seq",
+           "events_from_seq_batch"]
+
+
+def __getattr__(name):
+    if name in ("events_from_seq", "events_from_seq_batch", "prep_rf_simulation", "read_seq"):
+        from . import pulseq
+        return getattr(pulseq, name)
+    raise AttributeError(f"module {__name__!r} has no attribute {name!r}")
 
 #: Proton gyromagnetic ratio [rad / (s uT)]; /2pi gives 42.577 Hz/uT.
 GAMMA_RAD_PER_S_UT = 267.5153
