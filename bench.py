@@ -177,6 +177,12 @@ def cpu_baseline(P, M0, ev, n_cest, budget_s=15.0, kind="port"):
 
 
 # ------------------------------------------------------------------------------------------------
+# DRAM bytes per chain of chain_kernel from one ncu capture of a 2,048-voxel x 101-offset launch of the
+# default workload (27.2 MB read + 5,576.9 MB written, almost all of it register-spill traffic); it
+# grows with the number of chains a launch runs. Keyed by (CEST pools, precision, pulses).
+NCU_BYTES_PER_CHAIN = {(4, 0, 20): (27.224832e6 + 5.576863e9) / (2048 * 101)}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -281,6 +287,11 @@ def run_ours(args, rank, world, local_rank):
 
     achieved = flops / (ms * 1e-3) / 1e12
     value = world * nv / (ms * 1e-3)
+    traffic, traffic_src = None, "no ncu capture of this configuration"
+    if (nc, prec, args.pulses) in NCU_BYTES_PER_CHAIN:
+        traffic = NCU_BYTES_PER_CHAIN[(nc, prec, args.pulses)] * nv * n_off
+        traffic_src = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one 2,048-voxel launch, scaled by "
+                       "the chains of this launch (profiles/chain_kernel_forward_2048vox.md)")
     line = {
         "metric": "Z-spectra/s (batched forward simulation)", "value": value, "unit": "Z-spectra/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -296,7 +307,8 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
         "roofline": {"bound": "fp64-fma" if prec == _lib.F64 else "fp32-fma", "achieved": achieved,
                      "peak": best, "unit": "TFLOP/s", "frac": achieved / best if best else None,
-                     "traffic": None, "kernel": "chain_kernel",
+                     "traffic": traffic, "traffic_unit": "bytes per launch",
+                     "traffic_source": traffic_src, "kernel": "chain_kernel",
                      "flops_per_launch": flops, "taylor_terms": terms, "taylor_terms_executed": executed,
                      "dense_columns": hcols,
                      "dense_squarings": squar,

@@ -227,7 +227,7 @@ class DeviceEvents:
 
 def _device(a, dtype=np.float64):
     torch = _lib.torch_cuda()
-    return torch.as_tensor(np.ascontiguousarray(np.asarray(a, dtype))).to(torch.device("cuda"))
+    return torch.as_tensor(np.require(np.asarray(a, dtype), requirements=["C", "W"])).to(torch.device("cuda"))
 
 
 def problem(n_vox, n_off, n_ev, n_cest, mz, precision=None, reset_after_adc=True):
