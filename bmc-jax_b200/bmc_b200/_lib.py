@@ -24,7 +24,8 @@ SLOT_SPREAD_SIGMA, SLOT_M_START = -2, -3
 
 EXPORTS = ("bmc_abi_version", "bmc_version", "bmc_last_error", "bmc_release", "bmc_simulate",
            "bmc_simulate_jvp", "bmc_simulate_trajectory", "bmc_lm_fit", "bmc_normal_blocks",
-           "bmc_simulate_counted", "bmc_probe_fma_peak", "bmc_simulate_noalloc")
+           "bmc_simulate_counted", "bmc_probe_fma_peak", "bmc_simulate_noalloc", "bmc_mlp_sizes", "bmc_mlp_sync",
+           "bmc_mlp_forward", "bmc_mlp_backward", "bmc_mlp_adam_step")
 
 
 class Problem(C.Structure):
@@ -54,6 +55,10 @@ class FitSpecC(C.Structure):
                 ("scale", C.c_double * MAX_TANGENTS), ("lo", C.c_double * MAX_TANGENTS),
                 ("hi", C.c_double * MAX_TANGENTS), ("d_free", C.c_void_p),
                 ("n_points_skip", C.c_int32), ("reserved", C.c_int32)]
+
+
+class MlpShape(C.Structure):
+    _fields_ = [("n_in", C.c_int32), ("n_hidden", C.c_int32), ("n_hidden_layers", C.c_int32), ("n_out", C.c_int32)]
 
 
 _lib = None
@@ -92,6 +97,15 @@ def lib():
         L.bmc_probe_fma_peak.restype = C.c_int
         L.bmc_simulate_noalloc.argtypes = [C.POINTER(Problem), vp, C.POINTER(Events), vp, C.POINTER(Spread), vp, vp]
         L.bmc_simulate_noalloc.restype = C.c_int
+        sp, i64p = C.POINTER(MlpShape), C.POINTER(C.c_int64)
+        L.bmc_mlp_sizes.argtypes = [sp, C.c_int64, i64p, i64p, i64p]
+        L.bmc_mlp_sync.argtypes = [sp, vp, vp, vp]
+        L.bmc_mlp_forward.argtypes = [sp, vp, vp, vp, vp, vp, C.c_int64, vp, vp, C.c_int32, vp]
+        L.bmc_mlp_backward.argtypes = [sp, vp, vp, C.c_int64, vp, vp, vp, vp]
+        L.bmc_mlp_adam_step.argtypes = [sp, vp, vp, vp, vp, vp, C.c_int32, C.c_float, C.c_float, C.c_float,
+                                        C.c_float, vp]
+        for f in ("bmc_mlp_sizes", "bmc_mlp_sync", "bmc_mlp_forward", "bmc_mlp_backward", "bmc_mlp_adam_step"):
+            getattr(L, f).restype = C.c_int
         _lib = L
     return _lib
 

@@ -41,6 +41,18 @@ bmc_status fail(bmc_status s, const char* fmt, ...) {
         if (e_ != cudaSuccess) return fail(BMC_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(e_)); \
     } while (0)
 
+}  // namespace
+
+namespace bmc {
+// the same thread-local message for the library's other translation units (bmc_mlp.cu)
+bmc_status record_error(bmc_status s, const char* msg) {
+    g_err = msg;
+    return s;
+}
+}  // namespace bmc
+
+namespace {
+
 // ------------------------------------------------------------------------------------------------
 // truncated-Taylor tables: theta[m] = max t with t^(m+1)/(m+1)! e^t <= tol (forward bound on the
 // tail of exp, per sub-step), found by bisection

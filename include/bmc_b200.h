@@ -190,6 +190,47 @@ bmc_status bmc_simulate_noalloc(const bmc_problem* prob, const double* d_params,
                                 const double* d_m0, const bmc_spread* spread, double* d_out, void* stream);
 
 /*
+ * Learned warm start: a multilayer perceptron that maps a measured saturation ladder to normalised
+ * starting values for bmc_lm_fit, trained and evaluated with tcgen05 tensor-core GEMMs (bf16 inputs,
+ * fp32 accumulation). BMC-JAX has no learned component; these entry points are the
+ * bmc_mlp_{forward,backward,adam_step} of the build's boundary (starting values for
+ * fitting/independent.py:51-129, whose plain x0 stays the fallback).
+ *
+ * Network: x (n_in) -> n_hidden_layers x [affine, GELU (erf form)] of width n_hidden -> affine ->
+ * y (n_out). Every dimension is padded: in_pad = n_in rounded up to 64, out_pad = n_out rounded up
+ * to 64; n_hidden must be a multiple of 128 (<= 1024), n_out <= 128, 1..8 hidden layers.
+ * Parameters (d_params, float32, the master copy; also d_grad, d_m, d_v): for each layer l in order
+ * (hidden layers, then the output layer) W_l [out_l][in_l] row-major, then b_l [out_l], with
+ * in_0 = in_pad, in_l = n_hidden, out_l = n_hidden, out_L = out_pad; padded rows and columns must be
+ * zero (they then stay zero). The shadow (bf16, `shadow_bytes`) holds W_l and W_l^T per layer, as the
+ * tensor cores read them; bmc_mlp_sync rebuilds it from d_params and bmc_mlp_adam_step keeps it current.
+ * The work buffer (256-byte aligned, `work_bytes` for a batch size) holds the activations a backward
+ * pass needs; its first int32 is a status word: bit 0 is set when a GEMM gave up waiting for its
+ * tensor-core operations (about two seconds), and the caller clears it.
+ * Inputs x [batch][n_in] float32 are normalised as (x - d_in_shift[i]) * d_in_scale[i] (either may
+ * be NULL); outputs d_y [batch][n_out] float32 (may be NULL). Loss: mean over batch and outputs of
+ * (y - target)^2, added to *d_loss (may be NULL); gradients overwrite d_grad.
+ */
+typedef struct {
+    int32_t n_in;
+    int32_t n_hidden;
+    int32_t n_hidden_layers;
+    int32_t n_out;
+} bmc_mlp_shape;
+
+bmc_status bmc_mlp_sizes(const bmc_mlp_shape* shape, int64_t batch, int64_t* n_params, int64_t* shadow_bytes,
+                         int64_t* work_bytes);
+bmc_status bmc_mlp_sync(const bmc_mlp_shape* shape, const float* d_params, void* d_shadow, void* stream);
+bmc_status bmc_mlp_forward(const bmc_mlp_shape* shape, const float* d_params, const void* d_shadow,
+                           const float* d_x, const float* d_in_shift, const float* d_in_scale, int64_t batch,
+                           float* d_y, void* d_work, int32_t keep_for_backward, void* stream);
+bmc_status bmc_mlp_backward(const bmc_mlp_shape* shape, const void* d_shadow, const float* d_target, int64_t batch,
+                            void* d_work, float* d_grad, float* d_loss, void* stream);
+bmc_status bmc_mlp_adam_step(const bmc_mlp_shape* shape, float* d_params, const float* d_grad, float* d_m,
+                             float* d_v, void* d_shadow, int32_t step, float lr, float beta1, float beta2, float eps,
+                             void* stream);
+
+/*
  * Diagnostics (no counterpart in the reference: measurement support for the benchmark).
  * bmc_simulate_counted: bmc_simulate that also adds the work it executed to d_work[4] (device,
  *   zeroed by the caller): [0] Taylor sub-step terms each chain needed (one sparse operator product
