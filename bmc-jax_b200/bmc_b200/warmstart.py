@@ -224,6 +224,19 @@ class LadderWarmStart:
             out[a:b] = torch.as_tensor(np.asarray(z, np.float32)).to("cuda")
         return out
 
+    def simulate64(self, X_phys, chunk: int = 131072) -> np.ndarray:
+        """Z (float64, host) [n][n_points] of the Experiment with the free parameters set to X_phys."""
+        from .fitting import write_params
+        from .simulation import simulate_z, tile_params
+        X_phys = np.asarray(X_phys, np.float64)
+        ex = self.experiment
+        parts = []
+        for a in range(0, X_phys.shape[0], chunk):
+            b = min(a + chunk, X_phys.shape[0])
+            p = write_params(tile_params(ex.params, b - a), self.spec.to_scaled(X_phys[a:b]), self.spec)
+            parts.append(np.asarray(simulate_z(p, ex.events, ex.m0, ex.mz_loc), np.float64))
+        return np.concatenate(parts) if parts else np.zeros((0, self.n_points))
+
     def draw(self, n: int, seed: int) -> np.ndarray:
         """n parameter vectors drawn uniformly from the training ranges (physical units)."""
         rng = np.random.default_rng(seed)
