@@ -574,6 +574,52 @@ def within_1pct(x, truth, names):
     return ok
 
 
+def mlp_roofline(n_in, n_out, n_hidden=256, n_layers=3, batch=4096, steps=50, infer_batch=65536):
+    """Tensor-core rate of the warm-start network's kernels, timed with CUDA events on a fresh network
+    of the trained one's shape: training steps (forward with saved activations, backward, Adam) at
+    `batch`, and one inference pass at `infer_batch`. Algorithmic FLOPs per sample: forward
+    F = 2 (n_in H + (L-1) H^2 + H n_out); a training step 3F - 2 n_in H (every weight gradient, and
+    every input gradient but the first layer's)."""
+    import torch
+    from bmc_b200.warmstart import MLP
+    net = MLP(n_in, n_out, n_hidden, n_layers, seed=5)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    x = torch.rand((batch, n_in), generator=g, device="cuda")
+    t = torch.rand((batch, n_out), generator=g, device="cuda")
+    xi = torch.rand((infer_batch, n_in), generator=g, device="cuda")
+
+    def step():
+        net.forward(x, keep=True)
+        net.backward(t)
+        net.adam(1e-4)
+
+    for _ in range(5):
+        step()
+    net.forward(xi)
+    torch.cuda.synchronize()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    net.forward(xi)
+    e2.record()
+    e2.synchronize()
+    F = 2.0 * (n_in * n_hidden + (n_layers - 1) * n_hidden ** 2 + n_hidden * n_out)
+    train_tf = (3 * F - 2.0 * n_in * n_hidden) * batch * steps / (e0.elapsed_time(e1) * 1e-3) / 1e12
+    infer_tf = F * infer_batch / (e1.elapsed_time(e2) * 1e-3) / 1e12
+    peak = measured_peaks().get("bf16_tflops")
+    return {"bound": "tensor", "achieved": train_tf, "peak": peak, "unit": "TFLOP/s",
+            "frac": train_tf / peak if peak else None, "traffic": None,
+            "kernel": "gemm_kernel (tcgen05.mma kind::f16, bf16 in, fp32 TMEM accumulate)",
+            "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst cuBLAS GEMM)" if peak else "absent",
+            "train_step_ms": e0.elapsed_time(e1) / steps, "train_batch": batch,
+            "inference_tflops": infer_tf, "inference_ms": e1.elapsed_time(e2), "inference_batch": infer_batch,
+            # input kernel + (L + 1) GEMMs forward; loss kernel + 2 (L + 1) GEMMs backward; Adam
+            "gpu_launches_per_train_step": 3 * n_layers + 5}
+
+
 def run_warmfit(args, rank, world, local_rank):
     """Fitted voxels/s at <=1% parameter error, NN-warm vs plain LM: train the warm-start network on
     `--train` simulated ladders (noise sigma 0.005), then fit `--voxels` held-out noise-free voxels
@@ -617,6 +663,7 @@ def run_warmfit(args, rank, world, local_rank):
     ok_p = within_1pct(plain.x, X_true, names)
     ok_w = within_1pct(warm.x, X_true, names)
     x0_err = np.median(np.abs(warm.x0 / X_true - 1.0), axis=0)
+    roof = mlp_roofline(ws.n_points, spec.n)
     v_w = world * ok_w.sum() / warm_s
     v_p = world * ok_p.sum() / plain_s
     return {"metric": "fitted voxels/s at <=1% param err, NN-warm vs plain LM", "value": v_w, "unit": "voxels/s",
@@ -634,7 +681,8 @@ def run_warmfit(args, rank, world, local_rank):
                        "median_x0_rel_err": dict(zip(names, map(float, x0_err))),
                        "training": {"spectra": args.train, "epochs": args.epochs, "batch": 4096, "lr": 1e-3,
                                     "simulate_s": gen_s, "train_s": train_s, "loss_first_last": [hist[0], hist[-1]],
-                                    "noise_sigma": 0.005}}}
+                                    "noise_sigma": 0.005}},
+            "roofline": roof}
 
 
 def main():
