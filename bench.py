@@ -214,8 +214,18 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.current_stream(dev)
     sh = C.c_void_p(stream.cuda_stream)
 
+    sp, keep_sp, spread_cfg = None, None, None
+    if args.spread_nodes:
+        # configuration 5: every voxel a Gauss-Hermite B0 spread of sigma = 0.1 ppm at 3 T (12.77 Hz)
+        from bmc_b200.simulation import B0Spread
+        sigma_hz = 0.1 * 42.5764 * B0
+        u, w = B0Spread(sigma_hz, "gauss", args.spread_nodes).nodes_weights()
+        sig = torch.full((nv,), sigma_hz, dtype=torch.float64, device=dev)
+        sp, keep_sp = _lib.spread_struct(u, w, sig)
+        spread_cfg = {"shape": "gauss", "nodes": args.spread_nodes, "sigma_hz": sigma_hz}
+
     def step(params=dP, m0=dM, evs=dev_ev, out=dZ):
-        _lib.check(L.bmc_simulate(pr, C.c_void_p(params.data_ptr()), evs.struct, C.c_void_p(m0.data_ptr()), None,
+        _lib.check(L.bmc_simulate(pr, C.c_void_p(params.data_ptr()), evs.struct, C.c_void_p(m0.data_ptr()), sp,
                                   C.c_void_p(out.data_ptr()), sh))
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # 256 MB > L2 (126 MB)
@@ -226,7 +236,7 @@ def run_ours(args, rank, world, local_rank):
     # executed work of one launch (deterministic), from the kernel's own counters
     work = torch.zeros(4, dtype=torch.int64, device=dev)
     _lib.check(L.bmc_simulate_counted(pr, C.c_void_p(dP.data_ptr()), dev_ev.struct, C.c_void_p(dM.data_ptr()),
-                                      None, C.c_void_p(dZ.data_ptr()), C.c_void_p(work.data_ptr()), sh))
+                                      sp, C.c_void_p(dZ.data_ptr()), C.c_void_p(work.data_ptr()), sh))
     torch.cuda.synchronize(dev)
     terms, hcols, squar, executed = [int(x) for x in work.cpu()]
     nnz = 12 + 15 * nc                                   # nonzeros of A (+ C folded into term 1)
@@ -288,7 +298,7 @@ def run_ours(args, rank, world, local_rank):
     achieved = flops / (ms * 1e-3) / 1e12
     value = world * nv / (ms * 1e-3)
     traffic, traffic_src = None, "no ncu capture of this configuration"
-    if (nc, prec, args.pulses) in NCU_BYTES_PER_CHAIN:
+    if (nc, prec, args.pulses) in NCU_BYTES_PER_CHAIN and not args.spread_nodes:
         traffic = NCU_BYTES_PER_CHAIN[(nc, prec, args.pulses)] * nv * n_off
         traffic_src = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one 2,048-voxel launch, scaled by "
                        "the chains of this launch (profiles/chain_kernel_forward_2048vox.md)")
@@ -302,7 +312,7 @@ def run_ours(args, rank, world, local_rank):
                                f"20 Gaussian 50 ms pulses + 5 ms gaps, spoiler, 3 s recovery, ADC",
                    "voxels_per_gpu": nv, "offsets": n_off, "events": n_ev, "pools": nc,
                    "parallelism": f"dp{world} (voxels sharded, no collective)",
-                   "l2": "flushed between timed steps (256 MB write, untimed)"},
+                   "l2": "flushed between timed steps (256 MB write, untimed)", "b0_spread": spread_cfg},
         "e2e": {"value": world * nv / (e2e_ms * 1e-3), "unit": "Z-spectra/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
         "roofline": {"bound": "fp64-fma" if prec == _lib.F64 else "fp32-fma", "achieved": achieved,
@@ -316,7 +326,7 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clocks,
         "gpu_launches": 2 * args.steps,
     }
-    if rank == 0 and world == 1 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu and not args.spread_nodes:
         line["cpu_baseline"] = cpu_baseline(P, M0, ev, nc, budget_s=args.cpu_budget)
     return line
 
@@ -620,6 +630,75 @@ def mlp_roofline(n_in, n_out, n_hidden=256, n_layers=3, batch=4096, steps=50, in
             "gpu_launches_per_train_step": 3 * n_layers + 5}
 
 
+def dictionary_model():
+    """(base SimParams, 30-row saturation schedule, M0, mz, grid) of the dictionary configuration: water
+    + amide (3.5 ppm) + super-Lorentzian MT at 3 T; 30 rows, each a 1 s recovery, a 1 s CW block at the
+    amide offset with B1 0.5..6 uT (a seeded schedule) and the readout; the grid sweeps amide k
+    (64 log-spaced, 10..5000 1/s), amide f (32 log-spaced, 1e-5..0.02), water T1 (16, 0.8..2.5 s) and
+    rel_b1 (32, 0.7..1.3): 1,048,576 entries."""
+    from bmc_b200.simulation import SimEvent, SimParams, initial_state
+    p = SimParams(water_r1=np.float64(1 / 1.3), water_r2=np.float64(1 / 0.07), water_f=np.float64(1.0),
+                  cest_k=np.array([300.0]), cest_f=np.array([1e-3]), cest_dw=np.array([3.5]),
+                  cest_r1=np.array([1.0]), cest_r2=np.array([10.0]), mt_k=np.float64(30.0),
+                  mt_f=np.float64(0.05), mt_dw=np.float64(-2.5), mt_r1=np.float64(1.0), mt_r2=np.float64(1e5),
+                  mt_lineshape=np.int64(2), b0=np.float64(B0), gamma=np.float64(GAMMA),
+                  b0_inhom=np.float64(0.0), rel_b1=np.float64(1.0))
+    rng = np.random.default_rng(30)
+    b1 = rng.uniform(0.5, 6.0, 30)
+    n = b1.size
+    typ = np.tile(np.int32([0, 1, 3]), (n, 1))
+    dt = np.tile([1.0, 1.0, 0.0], (n, 1))
+    amp = np.stack([np.zeros(n), b1 * GAMMA / (2 * np.pi), np.zeros(n)], axis=1)
+    freq = np.stack([np.zeros(n), np.full(n, 3.5 * 42.5764 * B0), np.zeros(n)], axis=1)
+    ev = SimEvent(typ, dt, amp, np.zeros((n, 3)), freq, np.tile(np.int32([-1, -1, 0]), (n, 1)))
+    grid = {"cest_k": np.geomspace(10.0, 5000.0, 64), "cest_f": np.geomspace(1e-5, 0.02, 32),
+            "water_r1": 1.0 / np.linspace(0.8, 2.5, 16), "rel_b1": np.linspace(0.7, 1.3, 32)}
+    return p, ev, initial_state(p), 4, grid
+
+
+def run_dictionary(args, rank, world, local_rank):
+    """Dictionary entries/s through the public API (mrf.generate_dictionary, host fingerprints out),
+    then a 1% random subset of the entries against the float64 C oracle."""
+    import torch
+    from bmc_b200 import settings
+    from bmc_b200.mrf import build_param_grid, generate_dictionary
+    from bmc_b200.simulation import pack_params
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import bmc_oracle as O
+    torch.cuda.set_device(local_rank)
+    p, ev, m0, mz, grid = dictionary_model()
+    settings.use_x64(args.precision == "f64")
+    try:
+        generate_dictionary(p, ev, m0, {k: v[:2] for k, v in grid.items()}, mz)      # warm-up
+        torch.cuda.synchronize()
+        times = []
+        for _ in range(max(1, args.steps)):
+            t0 = time.perf_counter()
+            entries, fp = generate_dictionary(p, ev, m0, grid, mz, chunk_size=262144)
+            times.append(time.perf_counter() - t0)
+    finally:
+        settings.use_x64(True)
+    n = fp.shape[0]
+    s = float(np.median(times))
+    rng = np.random.default_rng(31)
+    pick = np.sort(rng.choice(n, max(1, n // 100), replace=False))
+    pb = build_param_grid(p, grid)
+    from bmc_b200.simulation import SimParams
+    sub = SimParams(*[np.asarray(v)[pick] for v in pb])
+    t0 = time.perf_counter()
+    want = O.c_simulate_z(pack_params(sub, pick.size), O.Events(*ev), np.broadcast_to(m0, (pick.size, m0.size)), 1, mz)
+    cpu_s = time.perf_counter() - t0
+    err = float(np.max(np.abs(fp[pick] - want)))
+    return {"metric": "dictionary entries/s (MRF dictionary, public API)", "value": world * n / s,
+            "unit": "entries/s", "n_gpus": world, "steps": len(times), "warmup": 1, "ms_per_step": s * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": args.precision,
+            "data": "synthetic grid", "config": {
+                "workload": f"MRF dictionary: {n} entries (k 64 x f 32 x T1 16 x rel_b1 32) x 30 saturation rows, "
+                            "water + amide + super-Lorentzian MT at 3 T, fingerprints to the host",
+                "subset_checked": int(pick.size), "subset_max_abs_err_vs_float64_oracle": err,
+                "cpu_oracle_entries_per_s": pick.size / cpu_s}}
+
+
 def run_warmfit(args, rank, world, local_rank):
     """Fitted voxels/s at <=1% parameter error, NN-warm vs plain LM: train the warm-start network on
     `--train` simulated ladders (noise sigma 0.005), then fit `--voxels` held-out noise-free voxels
@@ -691,11 +770,13 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["forward", "fit", "warmfit", "phantom08", "phantom09", "phantom10"],
+    ap.add_argument("--workload", choices=["forward", "fit", "warmfit", "dictionary", "phantom08", "phantom09",
+                                           "phantom10"],
                     default="forward")
     ap.add_argument("--train", type=int, default=2_000_000, help="warmfit: simulated training spectra")
     ap.add_argument("--epochs", type=int, default=10, help="warmfit: training epochs")
     ap.add_argument("--warm-iters", type=int, default=8, help="warmfit: LM iterations from the network's x0")
+    ap.add_argument("--spread-nodes", type=int, default=0, help="forward: B0-spread isochromats per voxel")
     ap.add_argument("--voxels", type=int, default=65536)
     ap.add_argument("--offsets", type=int, default=101)
     ap.add_argument("--pulses", type=int, default=20)
@@ -722,7 +803,7 @@ def main():
         if rank == 0:
             print(json.dumps(run_phantom(args)), flush=True)
         return
-    run = {"fit": run_fit, "warmfit": run_warmfit}.get(args.workload, run_ours)
+    run = {"fit": run_fit, "warmfit": run_warmfit, "dictionary": run_dictionary}.get(args.workload, run_ours)
     line = run(args, rank, world, local_rank)
     if rank == 0:
         print(json.dumps(line), flush=True)
