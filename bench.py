@@ -297,6 +297,18 @@ def run_ours(args, rank, world, local_rank):
 
     achieved = flops / (ms * 1e-3) / 1e12
     value = world * nv / (ms * 1e-3)
+    f32_err = None
+    if prec == _lib.F32:
+        # accuracy of the float32 kernel: the same voxels through the float64 kernel (after timing)
+        ns = min(nv, 4096)
+        z64 = torch.empty((ns, n_off), dtype=torch.float64, device=dev)
+        pr64 = problem(ns, n_off, n_ev, nc, mz, _lib.F64)
+        dP_s, dM_s = dP[:, :ns].contiguous(), dM[:ns].contiguous()
+        _lib.check(L.bmc_simulate(pr64, C.c_void_p(dP_s.data_ptr()), dev_ev.struct, C.c_void_p(dM_s.data_ptr()), sp,
+                                  C.c_void_p(z64.data_ptr()), sh))
+        step()
+        torch.cuda.synchronize(dev)
+        f32_err = {"voxels": ns, "max_abs_err_vs_f64": float((dZ[:ns] - z64).abs().max().item())}
     traffic, traffic_src = None, "no ncu capture of this configuration"
     if (nc, prec, args.pulses) in NCU_BYTES_PER_CHAIN and not args.spread_nodes:
         traffic = NCU_BYTES_PER_CHAIN[(nc, prec, args.pulses)] * nv * n_off
@@ -312,7 +324,8 @@ def run_ours(args, rank, world, local_rank):
                                f"20 Gaussian 50 ms pulses + 5 ms gaps, spoiler, 3 s recovery, ADC",
                    "voxels_per_gpu": nv, "offsets": n_off, "events": n_ev, "pools": nc,
                    "parallelism": f"dp{world} (voxels sharded, no collective)",
-                   "l2": "flushed between timed steps (256 MB write, untimed)", "b0_spread": spread_cfg},
+                   "l2": "flushed between timed steps (256 MB write, untimed)", "b0_spread": spread_cfg,
+                   "float32_accuracy": f32_err},
         "e2e": {"value": world * nv / (e2e_ms * 1e-3), "unit": "Z-spectra/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
         "roofline": {"bound": "fp64-fma" if prec == _lib.F64 else "fp32-fma", "achieved": achieved,
