@@ -25,7 +25,8 @@ SLOT_SPREAD_SIGMA, SLOT_M_START = -2, -3
 EXPORTS = ("bmc_abi_version", "bmc_version", "bmc_last_error", "bmc_release", "bmc_simulate",
            "bmc_simulate_jvp", "bmc_simulate_trajectory", "bmc_lm_fit", "bmc_normal_blocks",
            "bmc_simulate_counted", "bmc_probe_fma_peak", "bmc_simulate_noalloc", "bmc_mlp_sizes", "bmc_mlp_sync",
-           "bmc_mlp_forward", "bmc_mlp_backward", "bmc_mlp_adam_step")
+           "bmc_mlp_forward", "bmc_mlp_backward", "bmc_mlp_adam_step", "bmc_uneven_create", "bmc_uneven_simulate",
+           "bmc_uneven_destroy", "bmc_normal_segments", "bmc_schur_step")
 
 
 class Problem(C.Structure):
@@ -55,6 +56,11 @@ class FitSpecC(C.Structure):
                 ("scale", C.c_double * MAX_TANGENTS), ("lo", C.c_double * MAX_TANGENTS),
                 ("hi", C.c_double * MAX_TANGENTS), ("d_free", C.c_void_p),
                 ("n_points_skip", C.c_int32), ("reserved", C.c_int32)]
+
+
+class TableSet(C.Structure):
+    _fields_ = [("n_tables", C.c_int32), ("h_n_offsets", C.POINTER(C.c_int32)), ("h_n_events", C.POINTER(C.c_int32)),
+                ("ev", Events)]
 
 
 class MlpShape(C.Structure):
@@ -97,6 +103,16 @@ def lib():
         L.bmc_probe_fma_peak.restype = C.c_int
         L.bmc_simulate_noalloc.argtypes = [C.POINTER(Problem), vp, C.POINTER(Events), vp, C.POINTER(Spread), vp, vp]
         L.bmc_simulate_noalloc.restype = C.c_int
+        i32p = C.POINTER(C.c_int32)
+        L.bmc_uneven_create.argtypes = [C.c_int32, C.c_int32, i32p, C.POINTER(TableSet), C.c_int32, C.c_int32,
+                                        C.POINTER(C.c_void_p), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.bmc_uneven_simulate.argtypes = [vp, vp, vp, C.POINTER(Tangents), vp, vp, vp]
+        L.bmc_uneven_destroy.argtypes = [vp]
+        L.bmc_normal_segments.argtypes = [C.c_int32, C.c_int32, C.c_int64, vp, vp, vp, vp, vp, vp, vp]
+        L.bmc_schur_step.argtypes = [C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, C.c_double, vp, vp, vp, vp]
+        for f in ("bmc_uneven_create", "bmc_uneven_simulate", "bmc_uneven_destroy", "bmc_normal_segments",
+                  "bmc_schur_step"):
+            getattr(L, f).restype = C.c_int
         sp, i64p = C.POINTER(MlpShape), C.POINTER(C.c_int64)
         L.bmc_mlp_sizes.argtypes = [sp, C.c_int64, i64p, i64p, i64p]
         L.bmc_mlp_sync.argtypes = [sp, vp, vp, vp]

@@ -18,6 +18,7 @@
 #include <cub/device/device_radix_sort.cuh>
 
 #include "bmc_lm.cuh"
+#include "bmc_joint.cuh"
 
 using namespace bmc;
 
@@ -219,16 +220,17 @@ __global__ void __launch_bounds__(256) fma_probe_kernel(int iters, R seed, R* si
 // ------------------------------------------------------------------------------------------------
 // launches
 // ------------------------------------------------------------------------------------------------
-template <int NC, typename R, int NT>
+template <int NC, typename R, int NT, bool U = false>
 bmc_status launch_chain(const ChainArgs& a, const TaylorTable* tt, cudaStream_t st) {
     constexpr int kWarps = 4;
     const size_t smem = kWarps * sizeof(DenseSmem<NC, typename DenseReal<R>::type, NT>) +
                         32 * kWarps * sizeof(ChainConst<NC, Dn<R, NT>>);
-    CUDA_TRY(cudaFuncSetAttribute(chain_kernel<NC, R, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const long long nch = (long long)a.n_vox * a.n_off;
+    CUDA_TRY(cudaFuncSetAttribute(chain_kernel<NC, R, NT, U>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const long long nch = U ? a.n_chains : (long long)a.n_vox * a.n_off;
     const long long blocks = (nch + 127) / 128;
     if (blocks > 0x7fffffffLL) return fail(BMC_ERR_INVALID, "%lld chains exceed one launch", nch);
-    chain_kernel<NC, R, NT><<<(unsigned)blocks, kWarps * 32, smem, st>>>(a, tt);
+    if (blocks == 0) return BMC_OK;
+    chain_kernel<NC, R, NT, U><<<(unsigned)blocks, kWarps * 32, smem, st>>>(a, tt);
     CUDA_TRY(cudaGetLastError());
     return BMC_OK;
 }
@@ -265,21 +267,76 @@ size_t order_bytes(long long nch) {
 template <int NC>
 constexpr int tangents_per_pass() { return NC <= 1 ? 2 : 1; }
 
-template <int NC>
+template <int NC, bool U = false>
 bmc_status run_tangents(ChainArgs a, int P, const TaylorTable* tt, cudaStream_t st) {
     constexpr int TP = tangents_per_pass<NC>();
     for (int t0 = 0; t0 < P; t0 += TP) {
         a.t0 = t0;
-        bmc_status s = (P - t0 >= 2 && TP >= 2) ? launch_chain<NC, double, (TP >= 2 ? 2 : 1)>(a, tt, st)
-                                                : launch_chain<NC, double, 1>(a, tt, st);
+        bmc_status s = (P - t0 >= 2 && TP >= 2) ? launch_chain<NC, double, (TP >= 2 ? 2 : 1), U>(a, tt, st)
+                                                : launch_chain<NC, double, 1, U>(a, tt, st);
         if (s != BMC_OK) return s;
     }
     return BMC_OK;
 }
 
+// An uneven batch: voxels with their own event tables, one pool count. Owns its device buffers
+// (preprocessed records of every table, the chain map, the sort scratch); built by bmc_uneven_create.
+struct UnevenPlan {
+    int dev = 0, n_cest = 0, n_vox = 0, mz = 0, reset = 1, n_tables = 0;
+    long long n_chains = 0, n_rec = 0;
+    EvRec<double>* rec = nullptr;
+    int2* chain_map = nullptr;
+    int* vox_table = nullptr;
+    long long* tab_base = nullptr;
+    int* tab_noff = nullptr;
+    int* tab_nev = nullptr;
+    void* scratch = nullptr;   // sort keys and indices, cub scratch, status word
+    size_t scratch_bytes = 0;
+};
+
 template <int NC>
 struct Impl {
     static constexpr int N = Layout<NC>::N;
+
+    // one simulation (or tangent set) of an uneven batch: chains sorted by estimated cost, outputs
+    // in canonical chain order (voxel-major, then table row)
+    static bmc_status uneven(const UnevenPlan& pl, const double* params, const double* m0, const bmc_tangents* tg,
+                             double* z, double* jz, cudaStream_t st) {
+        const TaylorTable* tt = nullptr;
+        bmc_status s = tables(BMC_F64, &tt);
+        if (s != BMC_OK) return s;
+        ChainArgs a{};
+        a.n_vox = pl.n_vox; a.n_off = 1; a.n_ev = 0; a.n_fields = Layout<NC>::NF;
+        a.mz = pl.mz; a.reset_after_adc = pl.reset;
+        fill_spread(a, nullptr);
+        a.params = params; a.m0 = m0; a.out = z; a.jout = jz;
+        a.ev = pl.rec;
+        a.n_chains = pl.n_chains; a.chain_map = pl.chain_map; a.vox_table = pl.vox_table;
+        a.tab_base = pl.tab_base; a.tab_noff = pl.tab_noff; a.tab_nev = pl.tab_nev;
+        Carve cv(pl.scratch);
+        a.status = cv.take<int>(1);
+        CUDA_TRY(cudaMemsetAsync(a.status, 0, sizeof(int), st));
+        const long long nch = pl.n_chains;
+        if (nch >= 2 * 128) {
+            float* k_in = cv.take<float>(nch);
+            float* k_out = cv.take<float>(nch);
+            int* i_in = cv.take<int>(nch);
+            int* i_out = cv.take<int>(nch);
+            size_t tmp = 0;
+            CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp, k_in, k_out, i_in, i_out, (int)nch, 0, 32, st));
+            void* t = cv.take<char>(tmp);
+            if (cv.used > pl.scratch_bytes) return fail(BMC_ERR_INVALID, "uneven plan: scratch too small");
+            cost_kernel<NC, double, true><<<(unsigned)((nch + 127) / 128), 128, 0, st>>>(a, k_in, i_in);
+            CUDA_TRY(cudaGetLastError());
+            CUDA_TRY(cub::DeviceRadixSort::SortPairs(t, tmp, k_in, k_out, i_in, i_out, (int)nch, 0, 32, st));
+            a.order = i_out;
+        }
+        if (!tg) return launch_chain<NC, double, 0, true>(a, tt, st);
+        for (int t = 0; t < tg->n_tangents; ++t) a.field_row[t] = tg->field_row[t];
+        a.seed = tg->d_seed;
+        a.dm0 = tg->d_dm0;
+        return run_tangents<NC, true>(a, tg->n_tangents, tt, st);
+    }
 
     static bmc_status simulate(const bmc_problem* pr, const double* params, const bmc_events* ev, const double* m0,
                                const bmc_spread* sp, double* out, cudaStream_t st, unsigned long long* work = nullptr) {
@@ -575,6 +632,152 @@ bmc_status bmc_normal_blocks(int32_t n_voxels, int32_t n_points, int32_t n_tange
     if (!d_r || !d_jz || !d_H || !d_g || !d_c) return fail(BMC_ERR_INVALID, "normal blocks: null pointer");
     normal_blocks_kernel<<<(n_voxels + 3) / 4, 128, 0, (cudaStream_t)stream>>>(n_voxels, n_points, n_tangents, d_r,
                                                                                d_jz, d_H, d_g, d_c);
+    CUDA_TRY(cudaGetLastError());
+    return BMC_OK;
+}
+
+bmc_status bmc_uneven_create(int32_t n_cest, int32_t n_voxels, const int32_t* h_voxel_table,
+                             const bmc_table_set* tabs, int32_t mz_loc, int32_t reset_after_adc, void** plan,
+                             int64_t* n_chains, int64_t* h_chain_start) {
+    if (!plan) return fail(BMC_ERR_INVALID, "uneven: null plan pointer");
+    *plan = nullptr;
+    if (n_cest < 0 || n_cest > BMC_MAX_CEST) return fail(BMC_ERR_UNSUPPORTED, "n_cest %d outside 0..%d", n_cest, BMC_MAX_CEST);
+    if (n_voxels < 1 || !h_voxel_table || !tabs || tabs->n_tables < 1 || !tabs->h_n_offsets || !tabs->h_n_events)
+        return fail(BMC_ERR_INVALID, "uneven: voxels, their tables and the table sizes are required");
+    const int N = 3 * (1 + n_cest) + 1;
+    if (mz_loc < 0 || mz_loc >= N) return fail(BMC_ERR_INVALID, "mz_loc %d outside the state (size %d)", mz_loc, N);
+    const int nt = tabs->n_tables;
+    std::vector<long long> base(nt);
+    long long nrec = 0;
+    for (int t = 0; t < nt; ++t) {
+        if (tabs->h_n_offsets[t] < 1 || tabs->h_n_events[t] < 0)
+            return fail(BMC_ERR_INVALID, "uneven: table %d has %d rows and %d events", t, tabs->h_n_offsets[t],
+                        tabs->h_n_events[t]);
+        base[t] = nrec;
+        nrec += (long long)tabs->h_n_offsets[t] * tabs->h_n_events[t];
+    }
+    if (nrec > 0 && (!tabs->ev.d_type || !tabs->ev.d_dt || !tabs->ev.d_rf_amp || !tabs->ev.d_rf_phase ||
+                     !tabs->ev.d_rf_freq))
+        return fail(BMC_ERR_INVALID, "uneven: null event field");
+    std::vector<int2> cm;
+    std::vector<long long> start((size_t)n_voxels + 1);
+    for (int v = 0; v < n_voxels; ++v) {
+        const int t = h_voxel_table[v];
+        if (t < 0 || t >= nt) return fail(BMC_ERR_INVALID, "uneven: voxel %d names table %d of %d", v, t, nt);
+        start[v] = (long long)cm.size();
+        for (int o = 0; o < tabs->h_n_offsets[t]; ++o) cm.push_back(make_int2(v, o));
+    }
+    start[n_voxels] = (long long)cm.size();
+    const long long nch = (long long)cm.size();
+    if (nch > 0x7fffffffLL) return fail(BMC_ERR_INVALID, "uneven: %lld chains exceed one launch", nch);
+    UnevenPlan* pl = new UnevenPlan();
+    pl->n_cest = n_cest; pl->n_vox = n_voxels; pl->mz = mz_loc; pl->reset = reset_after_adc ? 1 : 0;
+    pl->n_tables = nt; pl->n_chains = nch; pl->n_rec = nrec;
+    auto undo = [&](bmc_status s) {
+        bmc_uneven_destroy(pl);
+        return s;
+    };
+    cudaError_t e = cudaGetDevice(&pl->dev);
+    std::vector<int> noff(tabs->h_n_offsets, tabs->h_n_offsets + nt), nev(tabs->h_n_events, tabs->h_n_events + nt);
+    pl->scratch_bytes = 256 + order_bytes(nch);
+    if (e == cudaSuccess) e = cudaMalloc(&pl->rec, sizeof(EvRec<double>) * std::max<long long>(nrec, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&pl->chain_map, sizeof(int2) * std::max<long long>(nch, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&pl->vox_table, sizeof(int) * n_voxels);
+    if (e == cudaSuccess) e = cudaMalloc(&pl->tab_base, sizeof(long long) * nt);
+    if (e == cudaSuccess) e = cudaMalloc(&pl->tab_noff, sizeof(int) * nt);
+    if (e == cudaSuccess) e = cudaMalloc(&pl->tab_nev, sizeof(int) * nt);
+    if (e == cudaSuccess) e = cudaMalloc(&pl->scratch, pl->scratch_bytes);
+    if (e == cudaSuccess && nch) e = cudaMemcpy(pl->chain_map, cm.data(), sizeof(int2) * nch, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(pl->vox_table, h_voxel_table, sizeof(int) * n_voxels, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(pl->tab_base, base.data(), sizeof(long long) * nt, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(pl->tab_noff, noff.data(), sizeof(int) * nt, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(pl->tab_nev, nev.data(), sizeof(int) * nt, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return undo(fail(BMC_ERR_CUDA, "uneven plan: %s", cudaGetErrorString(e)));
+    // every table's [n_offsets][n_events] arrays, concatenated in table order -> records [n_events][n_offsets]
+    for (int t = 0; t < nt; ++t) {
+        const size_t n = (size_t)noff[t] * nev[t];
+        if (!n) continue;
+        const long long b = base[t];
+        const int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+        prep_events_kernel<double><<<blocks, 256>>>(noff[t], nev[t], tabs->ev.d_type + b, tabs->ev.d_dt + b,
+                                                    tabs->ev.d_rf_amp + b, tabs->ev.d_rf_phase + b,
+                                                    tabs->ev.d_rf_freq + b, pl->rec + b);
+    }
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return undo(fail(BMC_ERR_CUDA, "uneven plan: %s", cudaGetErrorString(e)));
+    if (n_chains) *n_chains = nch;
+    if (h_chain_start) std::memcpy(h_chain_start, start.data(), sizeof(long long) * start.size());
+    *plan = pl;
+    return BMC_OK;
+}
+
+bmc_status bmc_uneven_simulate(const void* plan, const double* d_params, const double* d_m0,
+                               const bmc_tangents* tangents, double* d_z, double* d_jz, void* stream) {
+    if (!plan || !d_params || !d_m0 || !d_z) return fail(BMC_ERR_INVALID, "uneven: null plan, params, m0 or z");
+    const UnevenPlan* pl = static_cast<const UnevenPlan*>(plan);
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev != pl->dev) return fail(BMC_ERR_INVALID, "uneven: plan made on device %d, called on %d", pl->dev, dev);
+    if (tangents) {
+        const int nf = 13 + 5 * pl->n_cest;
+        if (tangents->n_tangents < 1 || tangents->n_tangents > BMC_MAX_TANGENTS || !tangents->d_seed || !d_jz)
+            return fail(BMC_ERR_INVALID, "uneven: 1..%d tangents with seeds and an output required", BMC_MAX_TANGENTS);
+        for (int t = 0; t < tangents->n_tangents; ++t)
+            if (tangents->field_row[t] < BMC_SEED_NONE || tangents->field_row[t] >= nf)
+                return fail(BMC_ERR_INVALID, "tangent %d: field row %d outside -1..%d", t, tangents->field_row[t], nf - 1);
+    }
+    BMC_DISPATCH(pl->n_cest, uneven(*pl, d_params, d_m0, tangents, d_z, d_jz, (cudaStream_t)stream));
+}
+
+bmc_status bmc_uneven_destroy(void* plan) {
+    UnevenPlan* pl = static_cast<UnevenPlan*>(plan);
+    if (!pl) return BMC_OK;
+    void* ptrs[] = {pl->rec, pl->chain_map, pl->vox_table, pl->tab_base, pl->tab_noff, pl->tab_nev, pl->scratch};
+    cudaError_t first = cudaSuccess;
+    for (void* p : ptrs) {
+        if (!p) continue;
+        const cudaError_t e = cudaFree(p);
+        if (first == cudaSuccess) first = e;
+    }
+    delete pl;
+    if (first != cudaSuccess) return fail(BMC_ERR_CUDA, "uneven plan: %s", cudaGetErrorString(first));
+    return BMC_OK;
+}
+
+bmc_status bmc_normal_segments(int32_t n_voxels, int32_t n_params, int64_t n_chains, const int64_t* d_chain_start,
+                               const double* d_jz, const double* d_r, double* d_H, double* d_g, double* d_c,
+                               void* stream) {
+    if (n_voxels < 1 || n_params < 1 || n_params > kMaxJointP || n_chains < 0)
+        return fail(BMC_ERR_INVALID, "normal segments: %d voxels, %d parameters (1..%d)", n_voxels, n_params, kMaxJointP);
+    if (!d_chain_start || !d_jz || !d_r || !d_H || !d_g || !d_c)
+        return fail(BMC_ERR_INVALID, "normal segments: null pointer");
+    const long long threads = (long long)n_voxels * 32;
+    normal_segments_kernel<<<(unsigned)((threads + 127) / 128), 128, 0, (cudaStream_t)stream>>>(
+        n_voxels, n_params, n_chains, reinterpret_cast<const long long*>(d_chain_start), d_jz, d_r, d_H, d_g, d_c);
+    CUDA_TRY(cudaGetLastError());
+    return BMC_OK;
+}
+
+bmc_status bmc_schur_step(int32_t n_voxels, int32_t n_local, int32_t n_shared, const double* d_H, const double* d_g,
+                          const double* d_free, double lam, double* d_dx_local, double* d_dx_shared, double* d_work,
+                          void* stream) {
+    if (n_voxels < 1 || n_local < 1 || n_local > kMaxJointP - 1 || (n_shared != 0 && n_shared != 1))
+        return fail(BMC_ERR_INVALID, "schur step: %d voxels, %d local (1..%d) and %d shared (0 or 1) values",
+                    n_voxels, n_local, kMaxJointP - 1, n_shared);
+    if (!d_H || !d_g || !d_dx_local || !d_dx_shared || !d_work) return fail(BMC_ERR_INVALID, "schur step: null pointer");
+    if (!(lam >= 0.0)) return fail(BMC_ERR_INVALID, "schur step: damping %g", lam);
+    const cudaStream_t st = (cudaStream_t)stream;
+    double* Y = d_work;
+    double* w = Y + (size_t)n_voxels * n_local;
+    double* red = w + (size_t)n_voxels * n_local;
+    schur_eliminate_kernel<<<(n_voxels + 127) / 128, 128, 0, st>>>(n_voxels, n_local, n_shared, d_H, d_g, d_free, lam,
+                                                                   Y, w, red);
+    CUDA_TRY(cudaGetLastError());
+    schur_reduce_kernel<<<1, 1024, 0, st>>>(n_voxels, n_shared, red, lam, d_dx_shared);
+    CUDA_TRY(cudaGetLastError());
+    const long long n = (long long)n_voxels * n_local;
+    schur_back_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(n_voxels, n_local, Y, w, d_dx_shared, d_dx_local);
     CUDA_TRY(cudaGetLastError());
     return BMC_OK;
 }

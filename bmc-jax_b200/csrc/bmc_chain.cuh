@@ -50,6 +50,13 @@ struct ChainArgs {
     int* status;               // error flags (bit 0: non-finite norm)
     unsigned long long* work;  // null, or [4]: useful Taylor terms, dense Horner column products,
                                // dense squarings, Taylor terms executed (warp maximum)
+    // uneven batches (chain_kernel<..., true>): every voxel has its own event table
+    long long n_chains;        // chains of the launch (canonical order: voxel-major, then row)
+    const int2* chain_map;     // [n_chains]: (voxel, row of its table)
+    const int* vox_table;      // [n_vox]: table of each voxel
+    const long long* tab_base; // [n_tables]: first record of each table in `ev`
+    const int* tab_noff;       // [n_tables]: rows (records per event) of each table
+    const int* tab_nev;        // [n_tables]: events of each table
 };
 
 template <int NC>

@@ -230,7 +230,7 @@ __device__ __forceinline__ void convert_flat(const A& a, B& b) {
 // ------------------------------------------------------------------------------------------------
 // the chain kernel
 // ------------------------------------------------------------------------------------------------
-template <int NC, typename R, int NT>
+template <int NC, typename R, int NT, bool UNEVEN = false>
 __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const ChainArgs a, const TaylorTable* __restrict__ ttab) {
     using D = Dn<R, NT>;
     using C = Chain<NC, R, NT>;
@@ -244,17 +244,32 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
 
     // chains in offset-fastest order: neighbouring lanes are neighbouring offsets of one voxel, so a
     // warp shares parameters and its chains need similar Taylor orders
-    const long long nch = (long long)a.n_vox * a.n_off;
+    const long long nch = UNEVEN ? a.n_chains : (long long)a.n_vox * a.n_off;
     long long ci = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = ci < nch;
     if (!valid) ci = nch - 1;
     if (a.order) ci = a.order[ci];                     // chains sorted by estimated cost (see cost_kernel)
-    const int v = (int)(ci / a.n_off), o = (int)(ci % a.n_off);
+    int v, o;
+    const EvRec<R>* __restrict__ ev = reinterpret_cast<const EvRec<R>*>(a.ev);
+    int stride = a.n_off, n_ev_own = a.n_ev, n_ev_loop = a.n_ev;
+    if constexpr (UNEVEN) {
+        // this chain's table: its records, row stride and length; the warp runs to its longest table
+        const int2 vm = a.chain_map[ci];
+        v = vm.x;
+        o = vm.y;
+        const int t = a.vox_table[v];
+        ev += a.tab_base[t];
+        stride = a.tab_noff[t];
+        n_ev_own = a.tab_nev[t];
+        n_ev_loop = (int)__reduce_max_sync(kFull, (unsigned)n_ev_own);
+    } else {
+        v = (int)(ci / a.n_off);
+        o = (int)(ci % a.n_off);
+    }
     const bool act = valid && (a.active == nullptr || a.active[v] != 0);
     if (__all_sync(kFull, !act)) return;
-    const EvRec<R>* __restrict__ ev = reinterpret_cast<const EvRec<R>*>(a.ev);
 
-    const size_t ch = (size_t)v * a.n_off + o;
+    const size_t ch = UNEVEN ? (size_t)ci : (size_t)v * a.n_off + o;
     unsigned long long wk0 = 0, wk1 = 0, wk2 = 0, wk3 = 0;
     const bool count = a.work != nullptr;
     ChainConst<NC, D>& cc = reinterpret_cast<ChainConst<NC, D>*>(smem_raw + 4 * sizeof(SM))[threadIdx.x];
@@ -269,8 +284,15 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
         bool reset_pending = false;
         R gkey = R(NAN);
         D gval = dconst<R, NT>(R(0));
-        for (int e = 0; e < a.n_ev; ++e) {
-            const EvRec<R> rec = ev[(size_t)e * a.n_off + o];
+        for (int e = 0; e < n_ev_loop; ++e) {
+            // past the end of its own table a lane sees an empty DELAY: no evolution, spoiler or readout
+            const bool in = !UNEVEN || e < n_ev_own;
+            EvRec<R> rec;
+            if (in) {
+                rec = ev[(size_t)e * stride + o];
+            } else {
+                rec.dt = R(0); rec.w1 = R(0); rec.c = R(1); rec.s = R(0); rec.wf = R(0); rec.type = R(EV_DELAY);
+            }
             if (reset_pending) {                                   // the ADC reset of the previous event
                 C::load_m0(a, v, M);
                 reset_pending = false;
@@ -331,12 +353,12 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
                 }
             }
             if (type == EV_GRADIENT || type == EV_SPOILER) C::spoil(M);
-            if (a.traj != nullptr && act) {
+            if (a.traj != nullptr && act && in) {
                 double* tp = a.traj + (ch * a.n_ev + e) * N;
 #pragma unroll
                 for (int q = 0; q < N; ++q) tp[q] = double(C::at(M, q).v);
             }
-            if (type == EV_ADC && a.reset_after_adc) reset_pending = (e + 1 < a.n_ev);
+            if (type == EV_ADC && a.reset_after_adc) reset_pending = (e + 1 < n_ev_own);
         }
         // last_M of this isochromat, weighted into the spread mean (written by the chain's own thread)
         if (act) {
@@ -351,7 +373,8 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
                     if (a.jout) {
 #pragma unroll
                         for (int t = 0; t < NT; ++t) {
-                            double* jp = a.jout + ((size_t)(a.t0 + t) * a.n_vox + v) * a.n_off + o;
+                            double* jp = UNEVEN ? a.jout + (size_t)(a.t0 + t) * a.n_chains + ch
+                                                : a.jout + ((size_t)(a.t0 + t) * a.n_vox + v) * a.n_off + o;
                             *jp = (node ? *jp : 0.0) + double(wgt * z.d[t]);
                         }
                     }
@@ -378,19 +401,31 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
 // cost estimate of every chain: the norm of its first RF event's generator (what sets its Taylor
 // order), so that chains of equal order can share a warp
 // ------------------------------------------------------------------------------------------------
-template <int NC, typename R>
+template <int NC, typename R, bool UNEVEN = false>
 __global__ void __launch_bounds__(128) cost_kernel(const ChainArgs a, float* __restrict__ key,
                                                    int* __restrict__ idx) {
     using C = Chain<NC, R, 0>;
     using D = Dn<R, 0>;
-    const long long nch = (long long)a.n_vox * a.n_off;
+    const long long nch = UNEVEN ? a.n_chains : (long long)a.n_vox * a.n_off;
     const long long ci = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (ci >= nch) return;
-    const int v = (int)(ci / a.n_off), o = (int)(ci % a.n_off);
     const EvRec<R>* __restrict__ ev = reinterpret_cast<const EvRec<R>*>(a.ev);
+    int v, o, stride = a.n_off, n_ev = a.n_ev;
+    if constexpr (UNEVEN) {
+        const int2 vm = a.chain_map[ci];
+        v = vm.x;
+        o = vm.y;
+        const int t = a.vox_table[v];
+        ev += a.tab_base[t];
+        stride = a.tab_noff[t];
+        n_ev = a.tab_nev[t];
+    } else {
+        v = (int)(ci / a.n_off);
+        o = (int)(ci % a.n_off);
+    }
     float cost = 0.f;
-    for (int e = 0; e < a.n_ev; ++e) {
-        const EvRec<R> rec = ev[(size_t)e * a.n_off + o];
+    for (int e = 0; e < n_ev; ++e) {
+        const EvRec<R> rec = ev[(size_t)e * stride + o];
         if ((int)rec.type != EV_RF || !(rec.dt > R(1e-9))) continue;
         ChainConst<NC, D> cc;
         C::load_const(a, v, 0, cc);

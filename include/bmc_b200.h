@@ -190,6 +190,53 @@ bmc_status bmc_simulate_noalloc(const bmc_problem* prob, const double* d_params,
                                 const double* d_m0, const bmc_spread* spread, double* d_out, void* stream);
 
 /*
+ * Uneven batches: voxels of one pool count with their own event tables (different offsets, pulse
+ * trains) in one launch. BMC-JAX expresses one event table per Experiment (fitting/experiment.py:43-46,
+ * fitting/joint.py:255), so an uneven batch is there one call per shape class; these entry points run
+ * the class mix at once and give every voxel the result its own class's call gives.
+ *   bmc_uneven_create: tables t = 0..n_tables-1 of h_n_offsets[t] x h_n_events[t] events, their six
+ *     arrays concatenated in table order in `ev` (device); h_voxel_table[v] names voxel v's table.
+ *     Builds the chain map (canonical order: voxel-major, then table row) and the tables' records on the
+ *     device (allocates; synchronises the device once). *n_chains = total rows; h_chain_start (host,
+ *     n_voxels + 1 entries, may be NULL) receives the first chain of every voxel.
+ *   bmc_uneven_simulate: d_params [13 + 5 n_cest][n_voxels], d_m0 [n_voxels][N]; d_z [n_chains] = state
+ *     mz_loc after each chain's last event; with tangents (field rows -1..n_fields-1, no spread),
+ *     d_jz [n_tangents][n_chains]. Replaces simulation/simulate.py:134-148 + voxels.py:89-129 per
+ *     shape class, and the jacfwd of fitting/joint.py:300,317.
+ */
+typedef struct {
+    int32_t n_tables;
+    const int32_t* h_n_offsets;    /* host [n_tables] */
+    const int32_t* h_n_events;     /* host [n_tables] */
+    bmc_events ev;                 /* device: the tables' arrays, concatenated */
+} bmc_table_set;
+
+bmc_status bmc_uneven_create(int32_t n_cest, int32_t n_voxels, const int32_t* h_voxel_table,
+                             const bmc_table_set* tables, int32_t mz_loc, int32_t reset_after_adc, void** plan,
+                             int64_t* n_chains, int64_t* h_chain_start);
+bmc_status bmc_uneven_simulate(const void* plan, const double* d_params, const double* d_m0,
+                               const bmc_tangents* tangents, double* d_z, double* d_jz, void* stream);
+bmc_status bmc_uneven_destroy(void* plan);
+
+/*
+ * The damped joint step with one value shared by every sample (fitting/joint.py:149-162's
+ * (H + lam (diag H + 1e-9 I)) d = -g, solved through the Schur complement of the shared column).
+ *   bmc_normal_segments: per voxel v, over its chains d_chain_start[v] .. d_chain_start[v+1]-1:
+ *     d_H [n_voxels][P][P] = J J^T, d_g [n_voxels][P] = J r, d_c [n_voxels] = r^T r, with
+ *     d_jz [P][n_chains] and d_r [n_chains]; P <= 9.
+ *   bmc_schur_step: P = n_local + n_shared (the shared column last, n_shared 0 or 1, n_local <= 8);
+ *     d_free [n_voxels][n_local] (1 free, 0 held; NULL = all free) -> d_dx_local [n_voxels][n_local],
+ *     d_dx_shared [1]. d_work holds (2 n_local + 4) n_voxels doubles. The shared sums are taken in a
+ *     fixed order (deterministic).
+ */
+bmc_status bmc_normal_segments(int32_t n_voxels, int32_t n_params, int64_t n_chains, const int64_t* d_chain_start,
+                               const double* d_jz, const double* d_r, double* d_H, double* d_g, double* d_c,
+                               void* stream);
+bmc_status bmc_schur_step(int32_t n_voxels, int32_t n_local, int32_t n_shared, const double* d_H, const double* d_g,
+                          const double* d_free, double lam, double* d_dx_local, double* d_dx_shared, double* d_work,
+                          void* stream);
+
+/*
  * Learned warm start: a multilayer perceptron that maps a measured saturation ladder to normalised
  * starting values for bmc_lm_fit, trained and evaluated with tcgen05 tensor-core GEMMs (bf16 inputs,
  * fp32 accumulation). BMC-JAX has no learned component; these entry points are the
