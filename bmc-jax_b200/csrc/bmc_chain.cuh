@@ -291,19 +291,22 @@ struct Chain {
                                                         int m_own, State<NC, D>& M,
                                                         const double* __restrict__ inv_fact,
                                                         const ChainConst<NC, D>& cst, R h) {
+        // The terms are added to M as they are formed (later terms derive from `term`, not from M), so no
+        // separate accumulator is held; a lane past its own sub-steps or degree adds with weight 0.
+        // fma(1, t, M) rounds like M + t and fma(0, t, M) is M: the result is that of summing apart.
 #pragma unroll 1
         for (int j = 0; j < ns_w; ++j) {
-            State<NC, D> term, acc = M;
+            const bool on = j < ns_own;
+            State<NC, D> term;
             matvec<true>(s, M, term, &cst, h);
-            axpy_state(acc, term);
+            fma_state(M, on ? R(1) : R(0), term);
 #pragma unroll 1
             for (int k = 2; k <= m_w; ++k) {
                 State<NC, D> nt;
                 matvec<false>(s, term, nt);
                 term = nt;
-                fma_state(acc, k <= m_own ? R(inv_fact[k]) : R(0), term);
+                fma_state(M, (on && k <= m_own) ? R(inv_fact[k]) : R(0), term);
             }
-            if (j < ns_own) M = acc;
         }
     }
 
