@@ -6,6 +6,7 @@
 // no host synchronisation inside a call).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -55,18 +56,19 @@ bmc_status record_error(bmc_status s, const char* msg) {
 namespace {
 
 // ------------------------------------------------------------------------------------------------
-// truncated-Taylor tables: theta[m] = max t with t^(m+1)/(m+1)! e^t <= tol (forward bound on the
-// tail of exp, per sub-step), found by bisection
+// truncated-Taylor tables: theta[m] = max t with t^(m+1)/(m+1)! / (1 - t/(m+2)) <= tol, a bound of the
+// tail sum_{k>m} t^k/k! of exp (each term at most t/(m+2) times the one before), per sub-step, found by
+// bisection
 // ------------------------------------------------------------------------------------------------
 TaylorTable make_table(double tol, int m_max, double dense_theta, double dense_switch) {
     TaylorTable t{};
     t.m_max = m_max;
     t.theta[0] = 0.0;
     for (int m = 1; m <= kTaylorMMax; ++m) {
-        double lo = 0.0, hi = 64.0;
+        double lo = 0.0, hi = std::min(64.0, (m + 2.0) * (1.0 - 1e-12));
         for (int it = 0; it < 200; ++it) {
             const double mid = 0.5 * (lo + hi);
-            const double lb = (m + 1) * std::log(mid) - std::lgamma(m + 2.0) + mid;
+            const double lb = (m + 1) * std::log(mid) - std::lgamma(m + 2.0) - std::log1p(-mid / (m + 2.0));
             if (lb <= std::log(tol)) lo = mid; else hi = mid;
         }
         t.theta[m] = lo;
