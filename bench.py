@@ -423,7 +423,8 @@ def run_fit(args, rank, world, local_rank):
 
 
 PHANTOM = ROOT / "tests" / "golden" / "phantom"
-PUBLISHED_S = {"phantom08": 15 * 60.0, "phantom09": 15 * 60.0, "phantom10": 2 * 3600.0}   # 1x RTX 3070
+PUBLISHED_S = {"phantom08": 15 * 60.0, "phantom09": 15 * 60.0, "phantom10": 2 * 3600.0,   # 1x RTX 3070
+               "phantom11": 3.5 * 3600.0}
 
 
 def phantom_data(tubes=None):
@@ -462,9 +463,10 @@ def phantom_events(stem, keep):
 
 
 def run_phantom(args):
-    """Tutorials 08 (QUESP fit), 09 (QUEST fit) and 10 (joint fit: shared water R2 factor, M_start and a
-    15-node B0 spread) of the reference on the shipped phantom data, through bmc_b200's public API; the
-    wall time of the fit call, host<->device traffic included, against the published RTX 3070 runtime."""
+    """Tutorials 08 (QUESP fit), 09 (QUEST fit), 10 (joint fit: shared water R2 factor, M_start and a
+    15-node B0 spread) and 11 (the joint fit again with one B1 factor per rung) of the reference on the
+    shipped phantom data, through bmc_b200's public API; the wall time of the fit calls, host<->device
+    traffic included, against the published RTX 3070 runtime."""
     import torch
     from dataclasses import replace
     from bmc_b200.fitting import Experiment, FitSpec, FreeParam, fit, fit_joint
@@ -499,7 +501,7 @@ def run_phantom(args):
            "rms_over_noise": (plain.rms / d6["noise_" + kind]).tolist(),
            "points": int(Z6.shape[1]), "events": lad6.n_events}
     value = t_plain
-    if w == "phantom10":
+    if w in ("phantom10", "phantom11"):
         d7 = phantom_data()
         pool = tuple(int(i) for i in np.flatnonzero(np.isfinite(d7["vial_dw"])))
         Kp, Fp, T2p = (replace(s, samples=pool) for s in (K, F, T2))
@@ -517,6 +519,18 @@ def run_phantom(args):
         value = t_plain + t_joint
         out.update(joint_s=t_joint, r2w=float(joint["r2w"][0]), m_start=float(joint["m_start"][0]),
                    sigma_hz=float(joint["sigma"][0]), joint_cost=[float(joint.cost[0]), float(joint.cost[-1])])
+        if w == "phantom11":
+            # tutorial 11: the same joint fit with one B1 factor per rung, shared by the tubes, from step 2
+            B1R = FreeParam("b1", "rel_b1", None, scale=1.0, lo=0.7, hi=1.3, x0=1.0, scope="block", mode="factor")
+            x1 = np.column_stack([joint.x, np.ones(joint.x.shape[0])])
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            rung = fit_joint(lad7, FitSpec([Kp, Fp, T2p, R2F, MS, SIG, B1R]), Z7, n_iter=12, n_per_block=n_per,
+                             x0_phys=x1, spread=B0Spread(nodes=15), block_jacobian="split")
+            t_rung = time.perf_counter() - t0
+            value += t_rung
+            out.update(rung_s=t_rung, b1_per_rung=np.asarray(rung.blocks["b1"]["x"]).reshape(-1).tolist(),
+                       rung_cost=[float(rung.cost[0]), float(rung.cost[-1])])
     pub = PUBLISHED_S[w]
     return {"metric": f"wall time of the reference's tutorial {w[-2:]} fit (public API, end to end)", "value": value,
             "unit": "s", "n_gpus": 1, "higher_is_better": False, "vs_baseline": value / pub,
@@ -870,7 +884,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["forward", "fit", "warmfit", "dictionary", "uneven", "phantom08",
-                                           "phantom09", "phantom10"],
+                                           "phantom09", "phantom10", "phantom11"],
                     default="forward")
     ap.add_argument("--train", type=int, default=2_000_000, help="warmfit: simulated training spectra")
     ap.add_argument("--epochs", type=int, default=10, help="warmfit: training epochs")

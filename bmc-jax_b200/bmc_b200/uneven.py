@@ -139,11 +139,15 @@ class UnevenFitResult:
 
 def fit_joint_uneven(batch: UnevenBatch, spec, z_meas: Sequence[np.ndarray], n_iter: int = 30,
                      x0_phys: Optional[np.ndarray] = None, x0_shared: Optional[float] = None, lam0: float = 1e-2,
-                     callback: Optional[Callable[[int, float], None]] = None) -> UnevenFitResult:
+                     callback: Optional[Callable[[int, float], None]] = None, group=None) -> UnevenFitResult:
     """Joint LM over an uneven batch: every `scope="sample"` slot free per voxel (where its field and pool
     exist), at most one `scope="shared"` slot common to all voxels; plain values only. z_meas[i] holds
     voxel i's measured Z (its table's rows). One damping for the whole problem, accept if the summed
-    squared residual falls (lam x 0.5) else lam x 3 (fitting/joint.py:149-162, 359-453)."""
+    squared residual falls (lam x 0.5) else lam x 3 (fitting/joint.py:149-162, 359-453).
+
+    `group`: a torch.distributed process group whose ranks each hold their own voxels (one GPU per
+    rank). The shared value is then common to the voxels of every rank: each iteration all-reduces four
+    numbers (the Schur sums of the shared column) and the costs, so every rank takes the same steps."""
     from .fitting import field_row
     torch = _lib.torch_cuda()
     loc = [l for l, s in enumerate(spec.slots) if s.scope == "sample"]
@@ -212,7 +216,20 @@ def fit_joint_uneven(batch: UnevenBatch, spec, z_meas: Sequence[np.ndarray], n_i
     H = torch.empty((n, P, P), dtype=torch.float64, device="cuda")
     gr = torch.empty((n, P), dtype=torch.float64, device="cuda")
     cv = torch.empty(n, dtype=torch.float64, device="cuda")
-    work = torch.empty((2 * PL + 4) * n, dtype=torch.float64, device="cuda")
+    work = torch.empty((2 * PL + 4) * n + 4, dtype=torch.float64, device="cuda")
+    sums = torch.empty(4, dtype=torch.float64, device="cuda")
+    if group is not None:
+        import torch.distributed as dist
+        allsum = lambda t: dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    else:
+        allsum = None
+
+    def total(v: float) -> float:
+        if allsum is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        allsum(t)
+        return float(t.item())
     d_loc = torch.empty((n, PL), dtype=torch.float64, device="cuda")
     d_s = torch.zeros(1, dtype=torch.float64, device="cuda")
     L = _lib.lib()
@@ -228,21 +245,28 @@ def fit_joint_uneven(batch: UnevenBatch, spec, z_meas: Sequence[np.ndarray], n_i
                                              _lib.ptr(r), _lib.ptr(Hg), _lib.ptr(gg), _lib.ptr(cg),
                                              _lib.stream_handle()))
             H[g.idx], gr[g.idx], cv[g.idx] = Hg, gg, cg
-        return float(cv.sum().item())
+        return total(float(cv.sum().item()))
 
     def cost_at(xl, xs, per_voxel=False):
         out = torch.empty(n, dtype=torch.float64, device="cuda")
         for g in batch.groups:
             r = g.run(params_at(g, xl, xs)) - g.zm
             out[g.idx] = torch.zeros(len(g.voxels), dtype=torch.float64, device="cuda").index_add_(0, g.seg, r * r)
-        return out if per_voxel else float(out.sum().item())
+        return out if per_voxel else total(float(out.sum().item()))
 
     lam = float(lam0)
     costs = []
     c = normal(x_loc, x_s)
     for it in range(int(n_iter)):
-        _lib.check(L.bmc_schur_step(n, PL, S, _lib.ptr(H), _lib.ptr(gr), _lib.ptr(d_free), lam, _lib.ptr(d_loc),
-                                    _lib.ptr(d_s), _lib.ptr(work), _lib.stream_handle()))
+        if allsum is None:
+            _lib.check(L.bmc_schur_step(n, PL, S, _lib.ptr(H), _lib.ptr(gr), _lib.ptr(d_free), lam, _lib.ptr(d_loc),
+                                        _lib.ptr(d_s), _lib.ptr(work), _lib.stream_handle()))
+        else:
+            _lib.check(L.bmc_schur_eliminate(n, PL, S, _lib.ptr(H), _lib.ptr(gr), _lib.ptr(d_free), lam,
+                                             _lib.ptr(work), _lib.ptr(sums), _lib.stream_handle()))
+            allsum(sums)
+            _lib.check(L.bmc_schur_back(n, PL, S, _lib.ptr(sums), lam, _lib.ptr(work), _lib.ptr(d_loc), _lib.ptr(d_s),
+                                        _lib.stream_handle()))
         xt = torch.minimum(torch.maximum(x_loc + d_loc, lo_l), hi_l)
         xst = float(np.clip(x_s + float(d_s.item()), lo[shr[0]], hi[shr[0]])) if S else 0.0
         ct = cost_at(xt, xst)

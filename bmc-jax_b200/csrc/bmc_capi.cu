@@ -91,6 +91,7 @@ __device__ TaylorTable g_tables[2];   // [BMC_F64, BMC_F32], per device
 
 struct DeviceState {
     bool tables_ready = false;
+    TaylorTable* tables = nullptr;   // device address of g_tables, taken once
     void* ws = nullptr;
     size_t ws_bytes = 0;
 };
@@ -111,11 +112,10 @@ bmc_status tables(int precision, const TaylorTable** out) {
         TaylorTable h[2] = {make_table(1e-13, 30, 0.5, 100.0),
                             make_table(std::ldexp(1.0, -24), 16, 0.5, 100.0)};
         CUDA_TRY(cudaMemcpyToSymbol(g_tables, h, sizeof(h)));
+        CUDA_TRY(cudaGetSymbolAddress((void**)&ds.tables, g_tables));
         ds.tables_ready = true;
     }
-    TaylorTable* p = nullptr;
-    CUDA_TRY(cudaGetSymbolAddress((void**)&p, g_tables));
-    *out = p + (precision == BMC_F32 ? 1 : 0);
+    *out = ds.tables + (precision == BMC_F32 ? 1 : 0);
     return BMC_OK;
 }
 
@@ -227,7 +227,16 @@ bmc_status launch_chain(const ChainArgs& a, const TaylorTable* tt, cudaStream_t 
     constexpr int kWarps = 4;
     const size_t smem = kWarps * sizeof(DenseSmem<NC, typename DenseReal<R>::type, NT>) +
                         32 * kWarps * sizeof(ChainConst<NC, Dn<R, NT>>);
-    CUDA_TRY(cudaFuncSetAttribute(chain_kernel<NC, R, NT, U>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // the attribute once per device and instantiation: later calls then only enqueue work (which keeps
+    // them capturable in a CUDA graph)
+    static unsigned long long configured = 0;
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev >= 64 || !((configured >> dev) & 1ull)) {
+        CUDA_TRY(cudaFuncSetAttribute(chain_kernel<NC, R, NT, U>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+        if (dev < 64) configured |= 1ull << dev;
+    }
     const long long nch = U ? a.n_chains : (long long)a.n_vox * a.n_off;
     const long long blocks = (nch + 127) / 128;
     if (blocks > 0x7fffffffLL) return fail(BMC_ERR_INVALID, "%lld chains exceed one launch", nch);
@@ -769,6 +778,20 @@ bmc_status bmc_schur_step(int32_t n_voxels, int32_t n_local, int32_t n_shared, c
                     n_voxels, n_local, kMaxJointP - 1, n_shared);
     if (!d_H || !d_g || !d_dx_local || !d_dx_shared || !d_work) return fail(BMC_ERR_INVALID, "schur step: null pointer");
     if (!(lam >= 0.0)) return fail(BMC_ERR_INVALID, "schur step: damping %g", lam);
+    double* sums = d_work + (size_t)n_voxels * (2 * n_local + 4);
+    bmc_status s = bmc_schur_eliminate(n_voxels, n_local, n_shared, d_H, d_g, d_free, lam, d_work, sums, stream);
+    if (s != BMC_OK) return s;
+    return bmc_schur_back(n_voxels, n_local, n_shared, sums, lam, d_work, d_dx_local, d_dx_shared, stream);
+}
+
+bmc_status bmc_schur_eliminate(int32_t n_voxels, int32_t n_local, int32_t n_shared, const double* d_H,
+                               const double* d_g, const double* d_free, double lam, double* d_work, double* d_sums,
+                               void* stream) {
+    if (n_voxels < 1 || n_local < 1 || n_local > kMaxJointP - 1 || (n_shared != 0 && n_shared != 1))
+        return fail(BMC_ERR_INVALID, "schur step: %d voxels, %d local (1..%d) and %d shared (0 or 1) values",
+                    n_voxels, n_local, kMaxJointP - 1, n_shared);
+    if (!d_H || !d_g || !d_work || !d_sums) return fail(BMC_ERR_INVALID, "schur step: null pointer");
+    if (!(lam >= 0.0)) return fail(BMC_ERR_INVALID, "schur step: damping %g", lam);
     const cudaStream_t st = (cudaStream_t)stream;
     double* Y = d_work;
     double* w = Y + (size_t)n_voxels * n_local;
@@ -776,7 +799,22 @@ bmc_status bmc_schur_step(int32_t n_voxels, int32_t n_local, int32_t n_shared, c
     schur_eliminate_kernel<<<(n_voxels + 127) / 128, 128, 0, st>>>(n_voxels, n_local, n_shared, d_H, d_g, d_free, lam,
                                                                    Y, w, red);
     CUDA_TRY(cudaGetLastError());
-    schur_reduce_kernel<<<1, 1024, 0, st>>>(n_voxels, n_shared, red, lam, d_dx_shared);
+    schur_sum_kernel<<<1, 1024, 0, st>>>(n_voxels, red, d_sums);
+    CUDA_TRY(cudaGetLastError());
+    return BMC_OK;
+}
+
+bmc_status bmc_schur_back(int32_t n_voxels, int32_t n_local, int32_t n_shared, const double* d_sums, double lam,
+                          const double* d_work, double* d_dx_local, double* d_dx_shared, void* stream) {
+    if (n_voxels < 1 || n_local < 1 || n_local > kMaxJointP - 1 || (n_shared != 0 && n_shared != 1))
+        return fail(BMC_ERR_INVALID, "schur step: %d voxels, %d local (1..%d) and %d shared (0 or 1) values",
+                    n_voxels, n_local, kMaxJointP - 1, n_shared);
+    if (!d_sums || !d_work || !d_dx_local || !d_dx_shared) return fail(BMC_ERR_INVALID, "schur step: null pointer");
+    if (!(lam >= 0.0)) return fail(BMC_ERR_INVALID, "schur step: damping %g", lam);
+    const cudaStream_t st = (cudaStream_t)stream;
+    const double* Y = d_work;
+    const double* w = Y + (size_t)n_voxels * n_local;
+    schur_shared_kernel<<<1, 32, 0, st>>>(n_shared, d_sums, lam, d_dx_shared);
     CUDA_TRY(cudaGetLastError());
     const long long n = (long long)n_voxels * n_local;
     schur_back_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(n_voxels, n_local, Y, w, d_dx_shared, d_dx_local);

@@ -177,10 +177,9 @@ __global__ void schur_eliminate_kernel(int n_vox, int PL, int S, const double* _
     if (v < n_vox) schur_eliminate_one(v, n_vox, PL, S, H, g, free, lam, Y, w, red);
 }
 
-// one block: the shared step ds = -(sum g_s - sum h_ps^T w) / (H_ss + lam (H_ss + 1e-9) - sum h_ps^T Y),
-// H_ss = sum h_ss; fixed summation order (deterministic)
-__global__ void schur_reduce_kernel(int n_vox, int S, const double* __restrict__ red, double lam,
-                                    double* __restrict__ ds) {
+// one block: the four Schur sums of a batch -- sum h_ss, sum h_ps^T Y, sum h_ps^T w, sum g_s -- in a
+// fixed order (deterministic); a sharded fit adds the batches' sums across ranks before the shared step
+__global__ void schur_sum_kernel(int n_vox, const double* __restrict__ red, double* __restrict__ sums) {
     __shared__ double sm[4][1024];
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     for (int v = threadIdx.x; v < n_vox; v += blockDim.x)
@@ -195,8 +194,13 @@ __global__ void schur_reduce_kernel(int n_vox, int S, const double* __restrict__
             for (int q = 0; q < 4; ++q) sm[q][threadIdx.x] += sm[q][threadIdx.x + s];
         __syncthreads();
     }
+    if (threadIdx.x < 4) sums[threadIdx.x] = sm[threadIdx.x][0];
+}
+
+// the shared step ds = -(sum g_s - sum h_ps^T w) / (H_ss + lam (H_ss + 1e-9) - sum h_ps^T Y), H_ss = sum h_ss
+__global__ void schur_shared_kernel(int S, const double* __restrict__ sums, double lam, double* __restrict__ ds) {
     if (threadIdx.x == 0) {
-        const double hss = sm[0][0], sy = sm[1][0], tw = sm[2][0], gs = sm[3][0];
+        const double hss = sums[0], sy = sums[1], tw = sums[2], gs = sums[3];
         ds[0] = S ? -(gs - tw) / (hss + lam * (hss + 1e-9) - sy) : 0.0;
     }
 }

@@ -226,8 +226,12 @@ bmc_status bmc_uneven_destroy(void* plan);
  *     d_jz [P][n_chains] and d_r [n_chains]; P <= 9.
  *   bmc_schur_step: P = n_local + n_shared (the shared column last, n_shared 0 or 1, n_local <= 8);
  *     d_free [n_voxels][n_local] (1 free, 0 held; NULL = all free) -> d_dx_local [n_voxels][n_local],
- *     d_dx_shared [1]. d_work holds (2 n_local + 4) n_voxels doubles. The shared sums are taken in a
- *     fixed order (deterministic).
+ *     d_dx_shared [1]. d_work holds (2 n_local + 4) n_voxels + 4 doubles. The shared sums are taken in
+ *     a fixed order (deterministic).
+ *   bmc_schur_eliminate + bmc_schur_back: the same step in two halves, for voxels sharded over several
+ *     GPUs. eliminate writes the per-voxel elimination into d_work ((2 n_local + 4) n_voxels doubles) and
+ *     this shard's four Schur sums into d_sums [4]; the caller adds d_sums over every shard (e.g. one
+ *     4-double all-reduce) and passes the total to back, which forms the shared step and each voxel's.
  */
 bmc_status bmc_normal_segments(int32_t n_voxels, int32_t n_params, int64_t n_chains, const int64_t* d_chain_start,
                                const double* d_jz, const double* d_r, double* d_H, double* d_g, double* d_c,
@@ -235,6 +239,11 @@ bmc_status bmc_normal_segments(int32_t n_voxels, int32_t n_params, int64_t n_cha
 bmc_status bmc_schur_step(int32_t n_voxels, int32_t n_local, int32_t n_shared, const double* d_H, const double* d_g,
                           const double* d_free, double lam, double* d_dx_local, double* d_dx_shared, double* d_work,
                           void* stream);
+bmc_status bmc_schur_eliminate(int32_t n_voxels, int32_t n_local, int32_t n_shared, const double* d_H,
+                               const double* d_g, const double* d_free, double lam, double* d_work, double* d_sums,
+                               void* stream);
+bmc_status bmc_schur_back(int32_t n_voxels, int32_t n_local, int32_t n_shared, const double* d_sums, double lam,
+                          const double* d_work, double* d_dx_local, double* d_dx_shared, void* stream);
 
 /*
  * Learned warm start: a multilayer perceptron that maps a measured saturation ladder to normalised

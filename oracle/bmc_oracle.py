@@ -573,3 +573,52 @@ def c_simulate_z(params_soa, ev: Events, m0, n_cest, mz, threads=0):
     L.oracle_simulate(nv, n_off, n_ev, n_cest, dp(P), t.ctypes.data_as(C.POINTER(C.c_int)), *[dp(a) for a in arr],
                       dp(m), int(mz), dp(out), int(threads))
     return out
+
+
+# ------------------------------------------------------------------------------------------------
+# the damped joint step with one shared value (fitting/joint.py:149-162), dense and by Schur complement
+# ------------------------------------------------------------------------------------------------
+def joint_step_dense(H, g, free, lam, S):
+    """Dense solve of (H + lam (diag H + 1e-9 I)) d = -g over every voxel's local values and (S = 1) one
+    value shared by all, assembled from per-voxel blocks H [n][P][P], g [n][P] (shared last), held
+    local values (free 0) with identity rows. Returns (d_local [n][PL], d_shared)."""
+    H, g, free = np.asarray(H, float), np.asarray(g, float), np.asarray(free, float)
+    n, P = g.shape
+    PL = P - S
+    dim = n * PL + S
+    A, b = np.zeros((dim, dim)), np.zeros(dim)
+    f = np.concatenate([free.ravel(), np.ones(S)])
+    for i in range(n):
+        idx = list(range(i * PL, (i + 1) * PL)) + ([n * PL] if S else [])
+        A[np.ix_(idx, idx)] += H[i]
+        b[idx] += g[i]
+    A = A * f[:, None] * f[None, :]
+    b = b * f
+    A = A + lam * (np.diag(np.diag(A)) + 1e-9 * np.eye(dim)) + np.diag(1.0 - f)
+    d = np.linalg.solve(A, -b)
+    return d[:n * PL].reshape(n, PL), (d[-1] if S else 0.0)
+
+
+def schur_partial(H, g, free, lam, S):
+    """One shard's part of the Schur-complement step: per voxel Y = A^-1 h_ps, w = A^-1 g_p, and the four
+    sums (h_ss, h_ps^T Y, h_ps^T w, g_s) over the shard's voxels."""
+    H, g, free = np.asarray(H, float), np.asarray(g, float), np.asarray(free, float)
+    n, P = g.shape
+    PL = P - S
+    Y, w, sums = np.zeros((n, PL)), np.zeros((n, PL)), np.zeros(4)
+    for i in range(n):
+        fr = free[i]
+        A = H[i, :PL, :PL] * np.outer(fr, fr) + np.diag(fr * lam * (np.diag(H[i, :PL, :PL]) + 1e-9) + (1 - fr))
+        hps = fr * H[i, :PL, PL] if S else np.zeros(PL)
+        Y[i] = np.linalg.solve(A, hps)
+        w[i] = np.linalg.solve(A, fr * g[i, :PL])
+        if S:
+            sums += [H[i, PL, PL], hps @ Y[i], hps @ w[i], g[i, PL]]
+    return Y, w, sums
+
+
+def schur_back(Y, w, sums, lam, S):
+    """The shared step from the sums of every shard, then each voxel's: (d_local, d_shared)."""
+    hss, sy, tw, gs = sums
+    ds = -(gs - tw) / (hss + lam * (hss + 1e-9) - sy) if S else 0.0
+    return -(w + Y * ds), ds

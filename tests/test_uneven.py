@@ -146,3 +146,44 @@ def test_joint_fit_recovers_the_truth(mixed):
     assert np.median(np.abs(res["k"] / truth_k - 1)) < 1e-3
     assert np.median(np.abs(res["r2w"] / truth_r2 - 1)) < 1e-4
     assert res.cost[-1] < 1e-3 * res.cost[0]
+
+
+def test_schur_step_in_one_call_and_in_shards_is_the_dense_step(cuda):
+    """bmc_schur_step, and bmc_schur_eliminate on two shards + summed sums + bmc_schur_back, against the
+    dense damped step of the whole problem (fitting/joint.py:149-162)."""
+    torch = cuda
+    from bmc_b200 import _lib
+    rng = np.random.default_rng(11)
+    n, PL, lam = 37, 4, 0.03
+    P = PL + 1
+    H = np.stack([(lambda J: J.T @ J)(rng.normal(size=(20, P))) for _ in range(n)])
+    g = rng.normal(size=(n, P))
+    free = np.ones((n, PL))
+    free[::4, 2] = 0.0
+    d_want, ds_want = O.joint_step_dense(H, g, free, lam, 1)
+    L = _lib.lib()
+    dev = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float64)).cuda()
+    dH, dg, dfree = dev(H), dev(g), dev(free)
+    d = torch.empty((n, PL), dtype=torch.float64, device="cuda")
+    ds = torch.empty(1, dtype=torch.float64, device="cuda")
+    work = torch.empty((2 * PL + 4) * n + 4, dtype=torch.float64, device="cuda")
+    _lib.check(L.bmc_schur_step(n, PL, 1, _lib.ptr(dH), _lib.ptr(dg), _lib.ptr(dfree), lam, _lib.ptr(d), _lib.ptr(ds),
+                                _lib.ptr(work), _lib.stream_handle()))
+    np.testing.assert_allclose(d.cpu().numpy(), d_want, rtol=1e-10, atol=1e-12)
+    assert float(ds.item()) == pytest.approx(ds_want, rel=1e-10)
+    # two shards
+    cut = 15
+    parts = [(slice(0, cut), cut), (slice(cut, n), n - cut)]
+    works = [torch.empty((2 * PL + 4) * m, dtype=torch.float64, device="cuda") for _, m in parts]
+    sums = [torch.empty(4, dtype=torch.float64, device="cuda") for _ in parts]
+    for (sl, m), wk, sm in zip(parts, works, sums):
+        _lib.check(L.bmc_schur_eliminate(m, PL, 1, _lib.ptr(dH[sl].contiguous()), _lib.ptr(dg[sl].contiguous()),
+                                         _lib.ptr(dfree[sl].contiguous()), lam, _lib.ptr(wk), _lib.ptr(sm),
+                                         _lib.stream_handle()))
+    total = sums[0] + sums[1]
+    for (sl, m), wk in zip(parts, works):
+        dd = torch.empty((m, PL), dtype=torch.float64, device="cuda")
+        _lib.check(L.bmc_schur_back(m, PL, 1, _lib.ptr(total), lam, _lib.ptr(wk), _lib.ptr(dd), _lib.ptr(ds),
+                                    _lib.stream_handle()))
+        np.testing.assert_allclose(dd.cpu().numpy(), d_want[sl], rtol=1e-10, atol=1e-12)
+    assert float(ds.item()) == pytest.approx(ds_want, rel=1e-10)
