@@ -106,7 +106,7 @@ def lib():
         i32p = C.POINTER(C.c_int32)
         L.bmc_uneven_create.argtypes = [C.c_int32, C.c_int32, i32p, C.POINTER(TableSet), C.c_int32, C.c_int32,
                                         C.POINTER(C.c_void_p), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
-        L.bmc_uneven_simulate.argtypes = [vp, vp, vp, C.POINTER(Tangents), vp, vp, vp]
+        L.bmc_uneven_simulate.argtypes = [vp, vp, vp, C.POINTER(Spread), C.POINTER(Tangents), vp, vp, vp]
         L.bmc_uneven_destroy.argtypes = [vp]
         L.bmc_normal_segments.argtypes = [C.c_int32, C.c_int32, C.c_int64, vp, vp, vp, vp, vp, vp, vp]
         L.bmc_schur_step.argtypes = [C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, C.c_double, vp, vp, vp, vp]

@@ -493,6 +493,12 @@ class _JointModel:
             self.blocks = [events]
         self.dev_blocks = [DeviceEvents(e) for e in self.blocks]
         self.rows, _ = _slot_rows(spec, self.nc)
+        # several blocks: every (sample, block) pair is one voxel of an uneven plan whose tables are the
+        # blocks, so that one launch covers all blocks (the blocks of a few samples would not fill the GPU)
+        self.merged = None
+        if nb > 1:
+            from .uneven import _Plan
+            self.merged = _Plan(self.nc, self.blocks, np.tile(np.arange(nb, dtype=np.int32), self.n), int(mz))
         self.mslot = next((l for l, s in enumerate(spec.slots) if s.field == "m_start"), None)
         self.sslot = next((l for l, s in enumerate(spec.slots) if s.field == "b0_spread"), None)
 
@@ -542,9 +548,51 @@ class _JointModel:
             seeds[self.sslot] = np.where(self.free[:, self.sslot], spec.slots[self.sslot].scale, 0.0)
         return q, m, sig, seeds, dm0
 
+    def _evaluate_merged(self, loc, need_jac):
+        """evaluate() for several blocks in one launch: voxel i * nb + b is sample i seen through block b."""
+        torch = _lib.torch_cuda()
+        L, n, nb, N = self.spec.n, self.n, self.nb, self.N
+        per = [self._effective(loc, b) for b in range(nb)]
+        nf = 13 + 5 * self.nc
+        P_all = np.stack([pack_params(q, n) for q, *_ in per], axis=2).reshape(nf, n * nb)
+        M_all = np.stack([m for _, m, *_ in per], axis=1).reshape(n * nb, N)
+        pdev, mdev = _device(P_all), _device(M_all)
+        sp, keep = (None, None)
+        if self.spread is not None:
+            u, w = self.spread.nodes_weights()
+            sig_all = np.stack([np.broadcast_to(np.asarray(sig, np.float64), (n,)) for _, _, sig, _, _ in per], axis=1)
+            sdev = _device(sig_all.reshape(n * nb))
+            sp, keep = _lib.spread_struct(u, w, sdev)
+        plan = self.merged
+        n_per = self.n_pts // nb
+        if not need_jac:
+            z = plan.run(pdev, mdev, spread=sp).cpu().numpy()
+            del keep
+            return z.reshape(n, nb * n_per), None
+        tg = _lib.Tangents()
+        tg.n_tangents = L
+        for l in range(L):
+            tg.field_row[l] = (_lib.SEED_NONE if self.rows[l] == _lib.SLOT_M_START else self.rows[l])
+        seeds = _device(np.stack([sd for _, _, _, sd, _ in per], axis=2).reshape(L, n * nb))
+        ddm0 = (_device(np.stack([d for *_, d in per], axis=2).reshape(L, n * nb, N))
+                if self.mslot is not None else None)
+        tg.d_seed = seeds.data_ptr()
+        tg.d_dm0 = None if ddm0 is None else ddm0.data_ptr()
+        jz = torch.empty((L, plan.n_chains), dtype=torch.float64, device="cuda")
+        z = plan.run(pdev, mdev, tg, jz, sp).cpu().numpy()
+        jr = jz.cpu().numpy().reshape(L, n, nb, n_per)
+        J = np.zeros((n, self.n_pts, self.n_loc))
+        for l in range(L):
+            for b in range(nb):
+                J[:, b * n_per:(b + 1) * n_per, self.pos[l] + (b if self.is_block[l] else 0)] = jr[l, :, b, :]
+        del keep
+        return z.reshape(n, nb * n_per), J
+
     def evaluate(self, loc, need_jac=True):
         """Z (n, n_pts) and, with need_jac, the local Jacobian (n, n_pts, n_loc)."""
         torch = _lib.torch_cuda()
+        if self.merged is not None:
+            return self._evaluate_merged(loc, need_jac)
         L = self.spec.n
         Z = np.empty((self.n, self.n_pts))
         J = np.zeros((self.n, self.n_pts, self.n_loc)) if need_jac else None

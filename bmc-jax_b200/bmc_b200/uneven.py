@@ -34,25 +34,15 @@ def _table_key(ev):
     return h.digest()
 
 
-class _Group:
-    """The voxels of one pool count: their packed parameters and start states on the device and the
-    library's plan (tables, chain map)."""
+class _Plan:
+    """The library's plan of one pool count: a set of event tables and the table of every voxel. `run`
+    simulates every voxel's chains (canonical order: voxel-major, then the rows of its table) in one
+    launch per tangent pass."""
 
-    def __init__(self, nc: int, voxels: List[int], experiments):
+    def __init__(self, nc: int, tables: Sequence, vox_table: np.ndarray, mz: int):
         torch = _lib.torch_cuda()
-        self.nc, self.voxels = nc, np.asarray(voxels, np.int64)
-        exps = [experiments[i] for i in voxels]
-        self.mz = int(exps[0].mz_loc)
-        if any(int(e.mz_loc) != self.mz for e in exps):
-            raise ValueError(f"voxels with {nc} CEST pools disagree on mz_loc")
-        keys, tables, vt = {}, [], []
-        for e in exps:
-            k = _table_key(e.events)
-            if k not in keys:
-                keys[k] = len(tables)
-                tables.append(e.events)
-            vt.append(keys[k])
-        self.vox_table = np.asarray(vt, np.int32)
+        self.nc, self.mz = int(nc), int(mz)
+        self.vox_table = np.ascontiguousarray(vox_table, np.int32)
         self.n_rows = np.array([np.shape(t.dt)[0] for t in tables], np.int32)
         n_ev = np.array([np.shape(t.dt)[1] for t in tables], np.int32)
         cat = lambda f, dt: np.concatenate([np.asarray(getattr(t, f), dt).reshape(-1) for t in tables])
@@ -61,27 +51,23 @@ class _Group:
               [torch.as_tensor(cat("adc_idx", np.int32)).cuda()]
         ts = _lib.TableSet(len(tables), self.n_rows.ctypes.data_as(C.POINTER(C.c_int32)),
                            n_ev.ctypes.data_as(C.POINTER(C.c_int32)), _lib.Events(*[x.data_ptr() for x in dev]))
-        self.chain_start = np.zeros(len(voxels) + 1, np.int64)
+        nv = self.vox_table.size
+        self.chain_start = np.zeros(nv + 1, np.int64)
         nch = C.c_int64()
         plan = C.c_void_p()
-        _lib.check(_lib.lib().bmc_uneven_create(nc, len(voxels), self.vox_table.ctypes.data_as(C.POINTER(C.c_int32)),
+        _lib.check(_lib.lib().bmc_uneven_create(self.nc, nv, self.vox_table.ctypes.data_as(C.POINTER(C.c_int32)),
                                                 C.byref(ts), self.mz, 1, C.byref(plan), C.byref(nch),
                                                 self.chain_start.ctypes.data_as(C.POINTER(C.c_int64))))
         self.plan, self.n_chains = plan, int(nch.value)
         self.d_chain_start = torch.as_tensor(self.chain_start).cuda()
-        params = [e.params for e in exps]
-        from .simulation import SimParams
-        stacked = SimParams(*[np.stack([np.asarray(getattr(p, f), np.float64) for p in params])
-                              for f in SimParams._fields])
-        self.params = torch.as_tensor(pack_params(stacked, len(voxels))).cuda()
-        self.m0 = torch.as_tensor(np.stack([np.asarray(e.m0, np.float64) for e in exps])).cuda()
-        self.N = state_size(nc)
 
-    def run(self, params=None, tangents=None, jz=None):
+    def run(self, params, m0, tangents=None, jz=None, spread=None):
+        """z [n_chains] (device) for params [n_fields][n_voxels] and m0 [n_voxels][N] (device, float64);
+        with tangents, their derivatives into jz [n_tangents][n_chains]; `spread` a _lib.Spread or None."""
         torch = _lib.torch_cuda()
         z = torch.empty(self.n_chains, dtype=torch.float64, device="cuda")
-        p = self.params if params is None else params
-        _lib.check(_lib.lib().bmc_uneven_simulate(self.plan, _lib.ptr(p), _lib.ptr(self.m0),
+        _lib.check(_lib.lib().bmc_uneven_simulate(self.plan, _lib.ptr(params), _lib.ptr(m0),
+                                                  None if spread is None else C.byref(spread),
                                                   None if tangents is None else C.byref(tangents), _lib.ptr(z),
                                                   _lib.ptr(jz), _lib.stream_handle()))
         return z
@@ -93,6 +79,38 @@ class _Group:
                 self.plan = C.c_void_p()
         except Exception:
             pass
+
+
+class _Group:
+    """The voxels of one pool count: their packed parameters and start states on the device and the plan
+    of their tables."""
+
+    def __init__(self, nc: int, voxels: List[int], experiments):
+        torch = _lib.torch_cuda()
+        self.nc, self.voxels = nc, np.asarray(voxels, np.int64)
+        exps = [experiments[i] for i in voxels]
+        mz = int(exps[0].mz_loc)
+        if any(int(e.mz_loc) != mz for e in exps):
+            raise ValueError(f"voxels with {nc} CEST pools disagree on mz_loc")
+        keys, tables, vt = {}, [], []
+        for e in exps:
+            k = _table_key(e.events)
+            if k not in keys:
+                keys[k] = len(tables)
+                tables.append(e.events)
+            vt.append(keys[k])
+        self.plan = _Plan(nc, tables, np.asarray(vt, np.int32), mz)
+        self.mz, self.chain_start, self.n_chains = mz, self.plan.chain_start, self.plan.n_chains
+        self.d_chain_start = self.plan.d_chain_start
+        from .simulation import SimParams
+        stacked = SimParams(*[np.stack([np.asarray(getattr(e.params, f), np.float64) for e in exps])
+                              for f in SimParams._fields])
+        self.params = torch.as_tensor(pack_params(stacked, len(voxels))).cuda()
+        self.m0 = torch.as_tensor(np.stack([np.asarray(e.m0, np.float64) for e in exps])).cuda()
+        self.N = state_size(nc)
+
+    def run(self, params=None, tangents=None, jz=None):
+        return self.plan.run(self.params if params is None else params, self.m0, tangents, jz)
 
 
 class UnevenBatch:

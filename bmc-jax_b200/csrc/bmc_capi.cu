@@ -311,15 +311,15 @@ struct Impl {
 
     // one simulation (or tangent set) of an uneven batch: chains sorted by estimated cost, outputs
     // in canonical chain order (voxel-major, then table row)
-    static bmc_status uneven(const UnevenPlan& pl, const double* params, const double* m0, const bmc_tangents* tg,
-                             double* z, double* jz, cudaStream_t st) {
+    static bmc_status uneven(const UnevenPlan& pl, const double* params, const double* m0, const bmc_spread* sp,
+                             const bmc_tangents* tg, double* z, double* jz, cudaStream_t st) {
         const TaylorTable* tt = nullptr;
         bmc_status s = tables(BMC_F64, &tt);
         if (s != BMC_OK) return s;
         ChainArgs a{};
         a.n_vox = pl.n_vox; a.n_off = 1; a.n_ev = 0; a.n_fields = Layout<NC>::NF;
         a.mz = pl.mz; a.reset_after_adc = pl.reset;
-        fill_spread(a, nullptr);
+        if ((s = fill_spread(a, sp)) != BMC_OK) return s;
         a.params = params; a.m0 = m0; a.out = z; a.jout = jz;
         a.ev = pl.rec;
         a.n_chains = pl.n_chains; a.chain_map = pl.chain_map; a.vox_table = pl.vox_table;
@@ -724,7 +724,8 @@ bmc_status bmc_uneven_create(int32_t n_cest, int32_t n_voxels, const int32_t* h_
 }
 
 bmc_status bmc_uneven_simulate(const void* plan, const double* d_params, const double* d_m0,
-                               const bmc_tangents* tangents, double* d_z, double* d_jz, void* stream) {
+                               const bmc_spread* spread, const bmc_tangents* tangents, double* d_z, double* d_jz,
+                               void* stream) {
     if (!plan || !d_params || !d_m0 || !d_z) return fail(BMC_ERR_INVALID, "uneven: null plan, params, m0 or z");
     const UnevenPlan* pl = static_cast<const UnevenPlan*>(plan);
     int dev = 0;
@@ -734,11 +735,13 @@ bmc_status bmc_uneven_simulate(const void* plan, const double* d_params, const d
         const int nf = 13 + 5 * pl->n_cest;
         if (tangents->n_tangents < 1 || tangents->n_tangents > BMC_MAX_TANGENTS || !tangents->d_seed || !d_jz)
             return fail(BMC_ERR_INVALID, "uneven: 1..%d tangents with seeds and an output required", BMC_MAX_TANGENTS);
+        const int lo = spread ? BMC_SEED_SPREAD_SIGMA : BMC_SEED_NONE;
         for (int t = 0; t < tangents->n_tangents; ++t)
-            if (tangents->field_row[t] < BMC_SEED_NONE || tangents->field_row[t] >= nf)
-                return fail(BMC_ERR_INVALID, "tangent %d: field row %d outside -1..%d", t, tangents->field_row[t], nf - 1);
+            if (tangents->field_row[t] < lo || tangents->field_row[t] >= nf)
+                return fail(BMC_ERR_INVALID, "tangent %d: field row %d outside %d..%d", t, tangents->field_row[t], lo,
+                            nf - 1);
     }
-    BMC_DISPATCH(pl->n_cest, uneven(*pl, d_params, d_m0, tangents, d_z, d_jz, (cudaStream_t)stream));
+    BMC_DISPATCH(pl->n_cest, uneven(*pl, d_params, d_m0, spread, tangents, d_z, d_jz, (cudaStream_t)stream));
 }
 
 bmc_status bmc_uneven_destroy(void* plan) {

@@ -199,10 +199,11 @@ bmc_status bmc_simulate_noalloc(const bmc_problem* prob, const double* d_params,
  *     Builds the chain map (canonical order: voxel-major, then table row) and the tables' records on the
  *     device (allocates; synchronises the device once). *n_chains = total rows; h_chain_start (host,
  *     n_voxels + 1 entries, may be NULL) receives the first chain of every voxel.
- *   bmc_uneven_simulate: d_params [13 + 5 n_cest][n_voxels], d_m0 [n_voxels][N]; d_z [n_chains] = state
- *     mz_loc after each chain's last event; with tangents (field rows -1..n_fields-1, no spread),
- *     d_jz [n_tangents][n_chains]. Replaces simulation/simulate.py:134-148 + voxels.py:89-129 per
- *     shape class, and the jacfwd of fitting/joint.py:300,317.
+ *   bmc_uneven_simulate: d_params [13 + 5 n_cest][n_voxels], d_m0 [n_voxels][N], an optional B0 spread
+ *     (as for bmc_simulate, sigma per voxel); d_z [n_chains] = state mz_loc after each chain's last
+ *     event; with tangents (field rows -1..n_fields-1, and BMC_SEED_SPREAD_SIGMA with a spread),
+ *     d_jz [n_tangents][n_chains]. Replaces simulation/simulate.py:134-148 + voxels.py:89-129 +
+ *     spread.py:77-106 per shape class, and the jacfwd of fitting/joint.py:300,317.
  */
 typedef struct {
     int32_t n_tables;
@@ -215,7 +216,8 @@ bmc_status bmc_uneven_create(int32_t n_cest, int32_t n_voxels, const int32_t* h_
                              const bmc_table_set* tables, int32_t mz_loc, int32_t reset_after_adc, void** plan,
                              int64_t* n_chains, int64_t* h_chain_start);
 bmc_status bmc_uneven_simulate(const void* plan, const double* d_params, const double* d_m0,
-                               const bmc_tangents* tangents, double* d_z, double* d_jz, void* stream);
+                               const bmc_spread* spread, const bmc_tangents* tangents, double* d_z, double* d_jz,
+                               void* stream);
 bmc_status bmc_uneven_destroy(void* plan);
 
 /*

@@ -289,3 +289,25 @@ def test_config2_scale_subset_against_the_c_oracle(cuda):
     err = np.abs(z.cpu().numpy() - want).max()
     print(f"config-2 subset: max |dZ| = {err:.2e}")
     assert err < 1e-9
+
+
+def test_merged_block_evaluation_equals_the_per_block_launches(joint3):
+    """A fit with a per-block value runs every (sample, block) pair in one launch; its Z and Jacobian
+    equal those of one launch per block, with a B0 spread, a spread width and m_start among the slots."""
+    from bmc_b200.fitting import Experiment, FitSpec, FreeParam, fit_joint
+    from bmc_b200.simulation import B0Spread
+    p, jp, true, events, m0, z, ppm = joint3
+    slots = [FreeParam(**K), FreeParam(**F),
+             FreeParam("b1", "rel_b1", None, 1.0, 0.7, 1.3, 1.0, scope="block", mode="factor"),
+             FreeParam("sig", "b0_spread", None, 10.0, 0.0, 60.0, 10.0, scope="shared"),
+             FreeParam("m0", "m_start", None, 1.0, 0.1, 1.0, 0.9, scope="shared")]
+    d = fit_joint(Experiment(true, events, m0, p.mz_loc), FitSpec(slots), z, n_per_block=ppm.size,
+                  spread=B0Spread(nodes=5), _internals=True)
+    model = d["model"]
+    assert model.merged is not None
+    loc = d["locs"](d["x0"] + 0.01 * np.linspace(-1.0, 1.0, d["x0"].size))
+    Zm, Jm = model.evaluate(loc)
+    model.merged = None
+    Zb, Jb = model.evaluate(loc)
+    np.testing.assert_allclose(Zm, Zb, rtol=0, atol=1e-13)
+    np.testing.assert_allclose(Jm, Jb, rtol=1e-12, atol=1e-14)
