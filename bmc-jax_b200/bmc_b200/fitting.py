@@ -495,10 +495,15 @@ class _JointModel:
         self.rows, _ = _slot_rows(spec, self.nc)
         # several blocks: every (sample, block) pair is one voxel of an uneven plan whose tables are the
         # blocks, so that one launch covers all blocks (the blocks of a few samples would not fill the GPU)
+        # and with a B0 spread every isochromat is one such voxel too (the spread's nodes would otherwise run
+        # one after another inside each chain)
         self.merged = None
-        if nb > 1:
+        self.nodes = spread.nodes_weights() if spread is not None else (np.zeros(1), np.ones(1))
+        if nb > 1 or spread is not None:
             from .uneven import _Plan
-            self.merged = _Plan(self.nc, self.blocks, np.tile(np.arange(nb, dtype=np.int32), self.n), int(mz))
+            nn = self.nodes[0].size
+            self.merged = _Plan(self.nc, self.blocks,
+                                np.repeat(np.tile(np.arange(nb, dtype=np.int32), self.n), nn), int(mz))
         self.mslot = next((l for l, s in enumerate(spec.slots) if s.field == "m_start"), None)
         self.sslot = next((l for l, s in enumerate(spec.slots) if s.field == "b0_spread"), None)
 
@@ -549,44 +554,68 @@ class _JointModel:
         return q, m, sig, seeds, dm0
 
     def _evaluate_merged(self, loc, need_jac):
-        """evaluate() for several blocks in one launch: voxel i * nb + b is sample i seen through block b."""
+        """evaluate() in one launch: voxel ((i nb + b) nn + j) is sample i seen through block b at
+        isochromat j (b0_inhom + sigma u_j / (gamma b0 / 2 pi), weight w_j; spread.py:77-106), and Z is the
+        weighted sum over the isochromats in node order, as the kernel's own node loop forms it. The
+        tangent of the spread width becomes a b0_inhom tangent seeded with u_j / (gamma b0 / 2 pi)."""
         torch = _lib.torch_cuda()
         L, n, nb, N = self.spec.n, self.n, self.nb, self.N
+        u, wts = self.nodes
+        nn = u.size
+        Lay = lambda name: field_row(name, None, self.nc)
+        row_b0i = Lay("b0_inhom")
         per = [self._effective(loc, b) for b in range(nb)]
         nf = 13 + 5 * self.nc
-        P_all = np.stack([pack_params(q, n) for q, *_ in per], axis=2).reshape(nf, n * nb)
-        M_all = np.stack([m for _, m, *_ in per], axis=1).reshape(n * nb, N)
-        pdev, mdev = _device(P_all), _device(M_all)
-        sp, keep = (None, None)
-        if self.spread is not None:
-            u, w = self.spread.nodes_weights()
-            sig_all = np.stack([np.broadcast_to(np.asarray(sig, np.float64), (n,)) for _, _, sig, _, _ in per], axis=1)
-            sdev = _device(sig_all.reshape(n * nb))
-            sp, keep = _lib.spread_struct(u, w, sdev)
+        P = np.empty((nf, n, nb, nn))
+        M = np.empty((n, nb, nn, N))
+        seeds = np.zeros((L, n, nb, nn))
+        dm0 = np.zeros((L, n, nb, nn, N)) if self.mslot is not None else None
+        for b, (q, m, sig, sd, dm) in enumerate(per):
+            pk = pack_params(q, n)
+            g = (1.0 / 6.283185307179586) * (pk[Lay("gamma")] * pk[Lay("b0")])   # Hz per ppm, as the kernel forms it
+            sg = np.broadcast_to(np.asarray(sig if sig is not None else 0.0, np.float64), (n,))
+            for j in range(nn):
+                P[:, :, b, j] = pk
+                P[row_b0i, :, b, j] = pk[row_b0i] + (u[j] * sg) / g
+                M[:, b, j] = m
+                seeds[:, :, b, j] = sd
+                if self.sslot is not None:
+                    seeds[self.sslot, :, b, j] = sd[self.sslot] * u[j] / g
+                if dm0 is not None:
+                    dm0[:, :, b, j] = dm
+        pdev = _device(P.reshape(nf, n * nb * nn))
+        mdev = _device(M.reshape(n * nb * nn, N))
         plan = self.merged
         n_per = self.n_pts // nb
+
+        def node_sum(a):                 # (..., n, nb, nn, n_per) -> weighted sum over nn, node order
+            acc = wts[0] * a[..., 0, :]
+            for j in range(1, nn):
+                acc = acc + wts[j] * a[..., j, :]
+            return acc
         if not need_jac:
-            z = plan.run(pdev, mdev, spread=sp).cpu().numpy()
-            del keep
-            return z.reshape(n, nb * n_per), None
+            z = plan.run(pdev, mdev).cpu().numpy().reshape(n, nb, nn, n_per)
+            return (node_sum(z) if nn > 1 else z[:, :, 0]).reshape(n, nb * n_per), None
         tg = _lib.Tangents()
         tg.n_tangents = L
         for l in range(L):
-            tg.field_row[l] = (_lib.SEED_NONE if self.rows[l] == _lib.SLOT_M_START else self.rows[l])
-        seeds = _device(np.stack([sd for _, _, _, sd, _ in per], axis=2).reshape(L, n * nb))
-        ddm0 = (_device(np.stack([d for *_, d in per], axis=2).reshape(L, n * nb, N))
-                if self.mslot is not None else None)
-        tg.d_seed = seeds.data_ptr()
+            r = self.rows[l]
+            tg.field_row[l] = (_lib.SEED_NONE if r == _lib.SLOT_M_START else
+                               (row_b0i if r == _lib.SLOT_SPREAD_SIGMA else r))
+        dseed = _device(seeds.reshape(L, n * nb * nn))
+        ddm0 = _device(dm0.reshape(L, n * nb * nn, N)) if dm0 is not None else None
+        tg.d_seed = dseed.data_ptr()
         tg.d_dm0 = None if ddm0 is None else ddm0.data_ptr()
         jz = torch.empty((L, plan.n_chains), dtype=torch.float64, device="cuda")
-        z = plan.run(pdev, mdev, tg, jz, sp).cpu().numpy()
-        jr = jz.cpu().numpy().reshape(L, n, nb, n_per)
+        z = plan.run(pdev, mdev, tg, jz).cpu().numpy().reshape(n, nb, nn, n_per)
+        jr = jz.cpu().numpy().reshape(L, n, nb, nn, n_per)
+        Z = node_sum(z) if nn > 1 else z[:, :, 0]
+        Jn = node_sum(jr) if nn > 1 else jr[:, :, :, 0]
         J = np.zeros((n, self.n_pts, self.n_loc))
         for l in range(L):
             for b in range(nb):
-                J[:, b * n_per:(b + 1) * n_per, self.pos[l] + (b if self.is_block[l] else 0)] = jr[l, :, b, :]
-        del keep
-        return z.reshape(n, nb * n_per), J
+                J[:, b * n_per:(b + 1) * n_per, self.pos[l] + (b if self.is_block[l] else 0)] = Jn[l, :, b, :]
+        return Z.reshape(n, nb * n_per), J
 
     def evaluate(self, loc, need_jac=True):
         """Z (n, n_pts) and, with need_jac, the local Jacobian (n, n_pts, n_loc)."""
