@@ -102,7 +102,7 @@ struct Dense {
     template <typename CC>
     static __device__ __noinline__ void event(SM* sm, int lane, bool evolve, const StepCoef<NC, D>& sc, const CC& cst,
                                               R dt, R nu, State<NC, D>& M, const TaylorTable& tt, int* status,
-                                              bool count, unsigned long long& wh, unsigned long long& ws) {
+                                              bool count, unsigned& wh, unsigned& ws) {
         const int grp = lane / GS, gl = lane % GS;
         unsigned need = __ballot_sync(kFull, evolve);
         while (need) {
@@ -132,8 +132,8 @@ struct Dense {
                 for (int i = 0; i < NC; ++i) sl->cc[i] = dconst<R, NT>(h) * cvt(cst.cc[i]);
                 sl->s = s;
                 if (count) {
-                    wh += (unsigned long long)NA * tt.dense_m;
-                    ws += (unsigned long long)s;
+                    wh += unsigned(NA * tt.dense_m);
+                    ws += unsigned(s);
                 }
 #pragma unroll
                 for (int q = 0; q < N; ++q) sl->vec[q] = C::at(M, q);
@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
     if (__all_sync(kFull, !act)) return;
 
     const size_t ch = UNEVEN ? (size_t)ci : (size_t)v * a.n_off + o;
-    unsigned long long wk0 = 0, wk1 = 0, wk2 = 0, wk3 = 0;
+    unsigned wk0 = 0, wk1 = 0, wk2 = 0, wk3 = 0;   // this chain's work counts (each < 2^32 per launch)
     const bool count = a.work != nullptr;
     ChainConst<NC, D>& cc = reinterpret_cast<ChainConst<NC, D>*>(smem_raw + 4 * sizeof(SM))[threadIdx.x];
     for (int node = 0; node < a.n_nodes; ++node) {
@@ -283,6 +283,7 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
         C::load_m0(a, v, M);
         bool reset_pending = false;
         R gkey = R(NAN);
+        int m_prev = 1;                                            // Taylor degree of the last event
         D gval = dconst<R, NT>(R(0));
         for (int e = 0; e < n_ev_loop; ++e) {
             // past the end of its own table a lane sees an empty DELAY: no evolution, spoiler or readout
@@ -338,18 +339,24 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
                 if (tay) {
                     const R thm = R(tt.theta[tt.m_max]);
                     ns_own = nu > thm ? (int)ceil(nu / thm) : 1;
-                    const R per = nu / R(ns_own);
-                    m_own = 1;
-                    while (m_own < tt.m_max && R(tt.theta[m_own]) < per) ++m_own;
+                    const R per = ns_own == 1 ? nu : nu / R(ns_own);
+                    // the smallest degree whose theta covers `per` (theta increases with m), searched from
+                    // the previous event's degree: consecutive events of a chain need similar degrees, so
+                    // this takes a step or two where a search from 1 takes m
+                    int m = m_prev;
+                    while (m < tt.m_max && R(tt.theta[m]) < per) ++m;
+                    while (m > 1 && R(tt.theta[m - 1]) >= per) --m;
+                    m_own = m;
+                    m_prev = m;
                 }
                 const int ns_w = __reduce_max_sync(kFull, (unsigned)ns_own);
                 const int m_w = __reduce_max_sync(kFull, (unsigned)m_own);
                 if (ns_w > 0) {
-                    const R h = tay ? rec.dt / R(ns_own) : R(0);
+                    const R h = tay ? (ns_own == 1 ? rec.dt : rec.dt / R(ns_own)) : R(0);
                     C::scale_coef(sc, h);
                     C::taylor_apply(sc, ns_w, m_w, ns_own, m_own, M, tt.inv_fact, cc, h);
-                    if (count && tay) wk0 += (unsigned long long)ns_own * m_own;
-                    if (count) wk3 += (unsigned long long)ns_w * m_w;
+                    if (count && tay) wk0 += unsigned(ns_own * m_own);
+                    if (count) wk3 += unsigned(ns_w * m_w);
                 }
             }
             if (type == EV_GRADIENT || type == EV_SPOILER) C::spoil(M);
@@ -389,7 +396,7 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
     if (a.work) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            unsigned long long x = act ? (q == 0 ? wk0 : (q == 1 ? wk1 : (q == 2 ? wk2 : wk3))) : 0ull;
+            unsigned long long x = act ? (unsigned long long)(q == 0 ? wk0 : (q == 1 ? wk1 : (q == 2 ? wk2 : wk3))) : 0ull;
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(kFull, x, off);
             if (lane == 0 && x) atomicAdd(a.work + q, x);
