@@ -185,22 +185,38 @@ struct Chain {
     // counts sqrt(R^2 + w^2) instead of R + w. Being an induced norm, it bounds ||X^k|| and so the
     // Taylor tail; the truncation error of water's entries stays below tol times max(|M_w|,
     // |M_c| / sqrt(f_c), 1).
-    static __device__ __forceinline__ R coef_norm(const StepCoef<NC, D>& s, const ChainConst<NC, D>& cc) {
+    //
+    // Every water and CEST row carries the RF term w1 once, so the bound is max(rows + w1, mt): `rows`
+    // (those rows without w1) and the MT row's constant depend on the event's frequency, not on its RF
+    // amplitude or phase, and a chain keeps them while its frequency stays the same (`NormBase`).
+    struct NormBase {
+        R rows;   // max over the water and CEST rows of their w1-free sums
+        R mt_c;   // the MT row without |R1 + k + w1^2 g|
+    };
+
+    static __device__ __forceinline__ NormBase norm_base(const StepCoef<NC, D>& s, const ChainConst<NC, D>& cc) {
         // the constant column C enters through the augmented row: |C_i| / d_i
-        const R w1 = hyp(fabs(s.w1x.v), fabs(s.w1y.v));
         R ex = R(0);
 #pragma unroll
         for (int i = 0; i < NC; ++i) ex += fabs(s.k[i].v) * R(cc.sf[i]);
-        R m = hyp(fabs(s.Rw2.v), fabs(s.offw.v)) + w1 + ex;
-        m = fmax(m, fabs(s.Rw1.v) + w1 + ex + fabs(s.kmt.v) * R(cc.sfm) + fabs(R(cc.cw.v)));
+        const R km = fabs(s.kmt.v) * R(cc.sfm);
+        R m = hyp(fabs(s.Rw2.v), fabs(s.offw.v)) + ex;
+        m = fmax(m, fabs(s.Rw1.v) + ex + km + fabs(R(cc.cw.v)));
 #pragma unroll
         for (int i = 0; i < NC; ++i) {
             const R b = fabs(s.k[i].v) * R(cc.sf[i]);
-            m = fmax(m, hyp(fabs(s.Rc2[i].v), fabs(s.offc[i].v)) + w1 + b);
-            m = fmax(m, fabs(s.Rc1[i].v) + w1 + b + fabs(R(cc.cc[i].v)) / R(cc.sf[i]));
+            m = fmax(m, hyp(fabs(s.Rc2[i].v), fabs(s.offc[i].v)) + b);
+            m = fmax(m, fabs(s.Rc1[i].v) + b + fabs(R(cc.cc[i].v)) / R(cc.sf[i]));
         }
-        m = fmax(m, fabs(s.Rm1W.v) + fabs(s.kmt.v) * R(cc.sfm) + fabs(R(cc.cm.v)) / R(cc.sfm));
-        return m;
+        return {m, km + fabs(R(cc.cm.v)) / R(cc.sfm)};
+    }
+
+    static __device__ __forceinline__ R rf_norm(const NormBase& b, R w1x, R w1y, R Rm1W) {
+        return fmax(b.rows + hyp(fabs(w1x), fabs(w1y)), fabs(Rm1W) + b.mt_c);
+    }
+
+    static __device__ __forceinline__ R coef_norm(const StepCoef<NC, D>& s, const ChainConst<NC, D>& cc) {
+        return rf_norm(norm_base(s, cc), s.w1x.v, s.w1y.v, s.Rm1W.v);
     }
 
     static __device__ __forceinline__ void scale_coef(StepCoef<NC, D>& s, R h) {

@@ -283,8 +283,16 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
         C::load_m0(a, v, M);
         bool reset_pending = false;
         R gkey = R(NAN);
-        int m_prev = 1;                                            // Taylor degree of the last event
+        // The Taylor degree of the last event and the range of sub-step norms it covers, (th_lo, th_hi]:
+        // an event whose norm falls in the same range takes the same degree without a table search.
+        int m_prev = 1;
+        R th_lo = R(-INFINITY), th_hi = tt.m_max > 1 ? R(tt.theta[1]) : R(INFINITY);
+        const R thm = R(tt.theta[tt.m_max]);
+        const bool mt_ls = cc.mt_on && cc.ls != 0;
         D gval = dconst<R, NT>(R(0));
+        // the frequency-dependent base of the norm bound, kept while the events' frequency stays fkey
+        R fkey = R(NAN);
+        typename C::NormBase nb{R(0), R(0)};
         for (int e = 0; e < n_ev_loop; ++e) {
             // past the end of its own table a lane sees an empty DELAY: no evolution, spoiler or readout
             const bool in = !UNEVEN || e < n_ev_own;
@@ -302,7 +310,7 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
             const bool evolve = act && rec.dt > R(1e-9);
             if (__any_sync(kFull, evolve)) {
                 D g = dconst<R, NT>(R(0));
-                if (cc.mt_on && cc.ls != 0 && rec.w1 != R(0)) {
+                if (mt_ls && rec.w1 != R(0)) {
                     if (rec.wf != gkey) {
                         gkey = rec.wf;
                         const D offmt = (rec.wf - cc.dw0) - cc.dwmt;
@@ -313,7 +321,11 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
                 }
                 StepCoef<NC, D> sc;
                 C::event_coef(cc, rec, g, sc);
-                R nu = evolve ? rec.dt * C::coef_norm(sc, cc) : R(0);
+                if (rec.wf != fkey) {
+                    nb = C::norm_base(sc, cc);
+                    fkey = rec.wf;
+                }
+                R nu = evolve ? rec.dt * C::rf_norm(nb, sc.w1x.v, sc.w1y.v, sc.Rm1W.v) : R(0);
                 if (!(nu < R(INFINITY))) {                          // NaN or inf: flag, let NaN propagate
                     if (evolve) atomicOr(a.status, 1);
                     nu = R(0);
@@ -337,17 +349,20 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
                 const bool tay = evolve && !dense_own;
                 int m_own = 0, ns_own = 0;
                 if (tay) {
-                    const R thm = R(tt.theta[tt.m_max]);
                     ns_own = nu > thm ? (int)ceil(nu / thm) : 1;
                     const R per = ns_own == 1 ? nu : nu / R(ns_own);
                     // the smallest degree whose theta covers `per` (theta increases with m), searched from
                     // the previous event's degree: consecutive events of a chain need similar degrees, so
                     // this takes a step or two where a search from 1 takes m
                     int m = m_prev;
-                    while (m < tt.m_max && R(tt.theta[m]) < per) ++m;
-                    while (m > 1 && R(tt.theta[m - 1]) >= per) --m;
+                    if (!(per > th_lo && per <= th_hi)) {
+                        while (m < tt.m_max && R(tt.theta[m]) < per) ++m;
+                        while (m > 1 && R(tt.theta[m - 1]) >= per) --m;
+                        m_prev = m;
+                        th_lo = m > 1 ? R(tt.theta[m - 1]) : R(-INFINITY);
+                        th_hi = m < tt.m_max ? R(tt.theta[m]) : R(INFINITY);
+                    }
                     m_own = m;
-                    m_prev = m;
                 }
                 const int ns_w = __reduce_max_sync(kFull, (unsigned)ns_own);
                 const int m_w = __reduce_max_sync(kFull, (unsigned)m_own);
