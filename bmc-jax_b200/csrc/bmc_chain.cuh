@@ -178,13 +178,17 @@ struct Chain {
 
     // sqrt(a^2 + b^2) <= max + (sqrt(2) - 1) min, within 8.3%
     static __device__ __forceinline__ R hyp(R a, R b) { return fmax(a, b) + R(0.41421357) * fmin(a, b); }
+    // sqrt(a^2 + b^2), rounded; the callers scale their result by (1 + kNormSlack) to keep a bound
+    static __device__ __forceinline__ R blk(R a, R b) { return sqrt(fma(a, a, b * b)); }
+    static constexpr double kNormSlack = sizeof(R) == 8 ? 1e-14 : 1e-6;
 
     // An upper bound of ||D^-1 A D|| in the norm max_b ||v_b||_2 / d_b over blocks b = (x, y) pairs and
     // z entries, with d = sqrt(f) per pool. The similarity balances the exchange terms (detailed
     // balance: k f one way, k the other, so k sqrt(f) both ways) and each precession-relaxation block
-    // counts sqrt(R^2 + w^2) instead of R + w. Being an induced norm, it bounds ||X^k|| and so the
-    // Taylor tail; the truncation error of water's entries stays below tol times max(|M_w|,
-    // |M_c| / sqrt(f_c), 1).
+    // counts sqrt(R^2 + w^2) instead of R + w (exactly in the part a chain keeps across events, through
+    // the bound `hyp` for the RF term, which changes every event). Being an induced norm, it bounds
+    // ||X^k|| and so the Taylor tail; the truncation error of water's entries stays below tol times
+    // max(|M_w|, |M_c| / sqrt(f_c), 1).
     //
     // Every water and CEST row carries the RF term w1 once, so the bound is max(rows + w1, mt): `rows`
     // (those rows without w1) and the MT row's constant depend on the event's frequency, not on its RF
@@ -200,15 +204,15 @@ struct Chain {
 #pragma unroll
         for (int i = 0; i < NC; ++i) ex += fabs(s.k[i].v) * R(cc.sf[i]);
         const R km = fabs(s.kmt.v) * R(cc.sfm);
-        R m = hyp(fabs(s.Rw2.v), fabs(s.offw.v)) + ex;
+        R m = blk(s.Rw2.v, s.offw.v) + ex;
         m = fmax(m, fabs(s.Rw1.v) + ex + km + fabs(R(cc.cw.v)));
 #pragma unroll
         for (int i = 0; i < NC; ++i) {
             const R b = fabs(s.k[i].v) * R(cc.sf[i]);
-            m = fmax(m, hyp(fabs(s.Rc2[i].v), fabs(s.offc[i].v)) + b);
+            m = fmax(m, blk(s.Rc2[i].v, s.offc[i].v) + b);
             m = fmax(m, fabs(s.Rc1[i].v) + b + fabs(R(cc.cc[i].v)) / R(cc.sf[i]));
         }
-        return {m, km + fabs(R(cc.cm.v)) / R(cc.sfm)};
+        return {m * R(1 + kNormSlack), (km + fabs(R(cc.cm.v)) / R(cc.sfm)) * R(1 + kNormSlack)};
     }
 
     static __device__ __forceinline__ R rf_norm(const NormBase& b, R w1x, R w1y, R Rm1W) {
