@@ -28,18 +28,32 @@ struct DenseGroup {
     static constexpr int NA = Layout<NC>::NA;
     static constexpr int GS = NA <= 8 ? 8 : (NA <= 16 ? 16 : 32);
     static constexpr int G = 32 / GS;
+    // column stride of the matrix in shared memory, odd: the lanes of a group store and read their
+    // columns (and rows) at element strides that fall on distinct banks
+    static constexpr int LD = NA | 1;
 };
 
 template <int NC, typename R, int NT>
-struct DenseSlot {
+struct DenseSlotBody {
     using D = Dn<R, NT>;
     static constexpr int NA = Layout<NC>::NA;
     StepCoef<NC, D> coef;           // the owner chain's coefficients, scaled by dt / 2^s
     D cw, cm, cc[NC > 0 ? NC : 1];  // ... and its constant column C, likewise scaled
-    D mat[NA * NA];                 // column-major: column j at [j * NA]
+    D mat[NA * DenseGroup<NC>::LD]; // column-major: column j at [j * LD]
     D vec[NA];                      // the owner's [M; 1]
     D out[NA];
     int s;
+};
+
+// A warp's G slots are read together (each group reads the same element of its own slot), so they are
+// padded to start 128 / G bytes apart modulo the 128-byte bank row: the G addresses of such a read fall
+// on different banks.
+template <int NC, typename R, int NT>
+struct DenseSlot : DenseSlotBody<NC, R, NT> {
+    static constexpr size_t kBody = sizeof(DenseSlotBody<NC, R, NT>);
+    static constexpr size_t kTarget = (128 / DenseGroup<NC>::G) % 128;
+    static constexpr size_t kPad = (kTarget + 128 - kBody % 128) % 128;
+    char pad[kPad == 0 ? 128 : kPad];
 };
 
 template <int NC, typename R, int NT>
@@ -73,6 +87,7 @@ struct Dense {
     using SL = DenseSlot<NC, R, NT>;
     static constexpr int GS = DenseGroup<NC>::GS;
     static constexpr int G = DenseGroup<NC>::G;
+    static constexpr int LD = DenseGroup<NC>::LD;
 
     // y = X_A v + C * caug: one column of X times a column of the matrix being built
     static __device__ __forceinline__ void matvec_aug(const SL* sl, const State<NC, D>& v, R caug,
@@ -164,8 +179,8 @@ struct Dense {
                 const bool sq = work && q < s;
                 if (sq) {
 #pragma unroll
-                    for (int i = 0; i < N; ++i) sl->mat[gl * NA + i] = C::at(col, i);
-                    sl->mat[gl * NA + N] = dconst<R, NT>(caug);
+                    for (int i = 0; i < N; ++i) sl->mat[gl * LD + i] = C::at(col, i);
+                    sl->mat[gl * LD + N] = dconst<R, NT>(caug);
                 }
                 __syncwarp();
                 if (sq) {
@@ -175,11 +190,11 @@ struct Dense {
                     for (int l = 0; l < N; ++l) {
                         const D w = C::at(col, l);
 #pragma unroll
-                        for (int i = 0; i < N; ++i) C::at(nc, i) = dfma(sl->mat[l * NA + i], w, C::at(nc, i));
+                        for (int i = 0; i < N; ++i) C::at(nc, i) = dfma(sl->mat[l * LD + i], w, C::at(nc, i));
                     }
                     if (caug != R(0)) {           // the augmented column also picks up T[:, aug]
 #pragma unroll
-                        for (int i = 0; i < N; ++i) C::at(nc, i) = C::at(nc, i) + sl->mat[N * NA + i];
+                        for (int i = 0; i < N; ++i) C::at(nc, i) = C::at(nc, i) + sl->mat[N * LD + i];
                     }
                     col = nc;
                 }
@@ -188,12 +203,12 @@ struct Dense {
             // M <- T [M; 1]
             if (work) {
 #pragma unroll
-                for (int i = 0; i < N; ++i) sl->mat[gl * NA + i] = C::at(col, i);
+                for (int i = 0; i < N; ++i) sl->mat[gl * LD + i] = C::at(col, i);
             }
             __syncwarp();
             if (grp_owner >= 0 && gl < N) {
                 D acc = dconst<R, NT>(R(0));
-                for (int j = 0; j < NA; ++j) acc = dfma(sl->mat[j * NA + gl], sl->vec[j], acc);
+                for (int j = 0; j < NA; ++j) acc = dfma(sl->mat[j * LD + gl], sl->vec[j], acc);
                 sl->out[gl] = acc;
             }
             __syncwarp();
