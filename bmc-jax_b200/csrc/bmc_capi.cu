@@ -60,7 +60,9 @@ namespace {
 // tail sum_{k>m} t^k/k! of exp (each term at most t/(m+2) times the one before), per sub-step, found by
 // bisection
 // ------------------------------------------------------------------------------------------------
-TaylorTable make_table(double tol, int m_max, double dense_theta, double dense_switch) {
+// f32_eps > 0: the Taylor terms of a degree-m warp whose bound theta[m]^k / k! is at most f32_eps are
+// formed in float32 (f32_from[m] = the first such k); f32_eps = 0: none are.
+TaylorTable make_table(double tol, int m_max, double dense_theta, double dense_switch, double f32_eps) {
     TaylorTable t{};
     t.m_max = m_max;
     t.theta[0] = 0.0;
@@ -78,6 +80,15 @@ TaylorTable make_table(double tol, int m_max, double dense_theta, double dense_s
         if (k > 0) f *= k;
         t.inv_fact[k] = 1.0 / f;
         t.inv_k[k] = k > 0 ? 1.0 / k : 0.0;
+        t.inv_fact_f[k] = float(t.inv_fact[k]);
+    }
+    for (int m = 0; m <= kTaylorMMax; ++m) {
+        int k0 = m + 1;
+        if (f32_eps > 0.0) {
+            k0 = 2;
+            while (k0 <= m && k0 * std::log(t.theta[m]) - std::lgamma(k0 + 1.0) > std::log(f32_eps)) ++k0;
+        }
+        t.f32_from[m] = k0;
     }
     t.dense_theta = dense_theta;
     int md = 1;
@@ -109,8 +120,8 @@ bmc_status tables(int precision, const TaylorTable** out) {
     std::lock_guard<std::mutex> lk(g_mu);
     DeviceState& ds = dev_state(dev);
     if (!ds.tables_ready) {
-        TaylorTable h[2] = {make_table(1e-13, 30, 0.5, 100.0),
-                            make_table(std::ldexp(1.0, -24), 16, 0.5, 100.0)};
+        TaylorTable h[2] = {make_table(1e-13, 30, 0.5, 100.0, 1e-8),
+                            make_table(std::ldexp(1.0, -24), 16, 0.5, 100.0, 0.0)};
         CUDA_TRY(cudaMemcpyToSymbol(g_tables, h, sizeof(h)));
         CUDA_TRY(cudaGetSymbolAddress((void**)&ds.tables, g_tables));
         ds.tables_ready = true;
@@ -873,7 +884,7 @@ bmc_status noalloc_setup(int precision, void** scratch, const TaylorTable** tt) 
         return fail(BMC_ERR_UNSUPPORTED, "bmc_simulate_noalloc: device %d above %d", dev, kNoAllocMaxDevices - 1);
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
     if (!g_noalloc_tables[dev]) {
-        TaylorTable h[2] = {make_table(1e-13, 30, 0.5, 100.0), make_table(std::ldexp(1.0, -24), 16, 0.5, 100.0)};
+        TaylorTable h[2] = {make_table(1e-13, 30, 0.5, 100.0, 1e-8), make_table(std::ldexp(1.0, -24), 16, 0.5, 100.0, 0.0)};
         CUDA_TRY(cudaMemcpyToSymbol(g_tables, h, sizeof(h)));
         g_noalloc_tables[dev] = true;
     }

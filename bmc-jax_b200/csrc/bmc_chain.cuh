@@ -7,6 +7,8 @@
 //     (simulate.py:105-114); the result is last_M after the final event (simulate.py:128-132).
 // The time step is exp([A C; 0 0] h)^s [M; 1]; see bmc_device.cuh for how it is evaluated.
 #pragma once
+#include <type_traits>
+
 #include "bmc_device.cuh"
 
 namespace bmc {
@@ -25,6 +27,10 @@ struct TaylorTable {
     double dense_theta;    // dense path: ||X / 2^s|| <= dense_theta ...
     int dense_m;           // ... with this Horner degree
     double dense_switch;   // warps whose largest ||X|| exceeds this take the dense path
+    // float64 kernels: for a warp of Taylor degree m, the terms from f32_from[m] on are below 1e-8 of
+    // the state (theta[m]^k / k! <= 1e-8) and are formed in float32 (> m: none)
+    int f32_from[kTaylorMMax + 1];
+    float inv_fact_f[kTaylorMMax + 1];  // 1 / k! in float32
 };
 
 struct ChainArgs {
@@ -223,6 +229,15 @@ struct Chain {
         return rf_norm(norm_base(s, cc), s.w1x.v, s.w1y.v, s.Rm1W.v);
     }
 
+    // the RF entries of an event's coefficients, unscaled, computed as event_coef computes them
+    static __device__ __forceinline__ void rf_coef(const ChainConst<NC, D>& cc, const EvRec<R>& e, D g_mt, D& w1x,
+                                                   D& w1y, D& Rm1W) {
+        const D w1 = e.w1 * cc.relb1;
+        w1x = e.c * w1;
+        w1y = e.s * w1;
+        Rm1W = cc.Rm1 + (w1 * w1) * g_mt;
+    }
+
     static __device__ __forceinline__ void scale_coef(StepCoef<NC, D>& s, R h) {
         s.Rw2 = h * s.Rw2; s.Rw1 = h * s.Rw1;
 #pragma unroll
@@ -302,32 +317,90 @@ struct Chain {
         }
     }
 
-    // exp(X)^s [M; 1] by s sub-steps of the degree-m Taylor polynomial (X already scaled by the
-    // sub-step): the unnormalised powers p_k = X^k [M; 1] are accumulated with weights 1/k!, so each
-    // term is one sparse operator product and one fused multiply-add per state entry.
+    // exp(X)^s [M; 1] by s sub-steps of the degree-m Taylor polynomial, X = [A C; 0 0] h: the
+    // unnormalised powers p_k = X^k [M; 1] are accumulated with weights 1/k!, so each term is one sparse
+    // operator product and one fused multiply-add per state entry. The coefficients (scaled by h) are
+    // formed at each sub-step, so that they are not held in registers across the rest of the event.
     // The loops run to the warp's largest (s, m); each chain uses only its own (ns_own, m_own), so a
     // chain's result never depends on which chains share its warp.
-    static __device__ __forceinline__ void taylor_apply(const StepCoef<NC, D>& s, int ns_w, int m_w, int ns_own,
-                                                        int m_own, State<NC, D>& M,
-                                                        const double* __restrict__ inv_fact,
-                                                        const ChainConst<NC, D>& cst, R h) {
+    //
+    // In the float64 kernel without tangents, the terms from tt.f32_from[m_w] on (each below 1e-8 of the
+    // state, in the balanced norm of coef_norm) are formed in float32 and summed in a float32
+    // accumulator that is added to M once per sub-step: their rounding, a few units of 2^-24 of terms
+    // below 1e-8, stays under 1e-14 of the state per event, below the truncation tolerance 1e-13.
+    static __device__ __forceinline__ void taylor_apply(const ChainConst<NC, D>& cst, const EvRec<R>& rec, D g_mt,
+                                                        R h, int ns_w, int m_w, int ns_own, int m_own,
+                                                        State<NC, D>& M, const TaylorTable& tt) {
+        constexpr bool kMixed = std::is_same<R, double>::value && NT == 0;
         // The terms are added to M as they are formed (later terms derive from `term`, not from M), so no
         // separate accumulator is held; a lane past its own sub-steps or degree adds with weight 0.
         // fma(1, t, M) rounds like M + t and fma(0, t, M) is M: the result is that of summing apart.
+        const int k32 = kMixed ? tt.f32_from[m_w] : m_w + 1;
 #pragma unroll 1
         for (int j = 0; j < ns_w; ++j) {
             const bool on = j < ns_own;
+            const int m_on = on ? m_own : 0;
+            StepCoef<NC, D> s;
+            event_coef(cst, rec, g_mt, s);
+            scale_coef(s, h);
             State<NC, D> term;
             matvec<true>(s, M, term, &cst, h);
             fma_state(M, on ? R(1) : R(0), term);
+            int k = 2;
 #pragma unroll 1
-            for (int k = 2; k <= m_w; ++k) {
+            for (; k <= m_w && k < k32; ++k) {
                 State<NC, D> nt;
                 matvec<false>(s, term, nt);
                 term = nt;
-                fma_state(M, (on && k <= m_own) ? R(inv_fact[k]) : R(0), term);
+                fma_state(M, k <= m_on ? R(tt.inv_fact[k]) : R(0), term);
+            }
+            if constexpr (kMixed) {
+                if (k <= m_w) {
+                    using C32 = Chain<NC, float, 0>;
+                    using F = Dn<float, 0>;
+                    StepCoef<NC, F> s32;
+                    State<NC, F> t32, a32;
+                    to_float(s, s32);
+                    to_float(term, t32);
+                    zero_state(a32);
+#pragma unroll 1
+                    for (; k <= m_w; ++k) {
+                        State<NC, F> n32;
+                        C32::template matvec<false>(s32, t32, n32);
+                        t32 = n32;
+                        C32::fma_state(a32, k <= m_on ? tt.inv_fact_f[k] : 0.f, t32);
+                    }
+                    add_float(M, a32);
+                }
             }
         }
+    }
+
+    // elementwise precision changes between structs made only of Dn<., 0> members (StepCoef, State)
+    template <typename A, typename B>
+    static __device__ __forceinline__ void to_float(const A& a, B& b) {
+        constexpr int n = sizeof(A) / sizeof(double);
+        static_assert(sizeof(B) == n * sizeof(float), "layouts differ");
+        const double* pa = reinterpret_cast<const double*>(&a);
+        float* pb = reinterpret_cast<float*>(&b);
+#pragma unroll
+        for (int i = 0; i < n; ++i) pb[i] = float(pa[i]);
+    }
+    template <typename B>
+    static __device__ __forceinline__ void zero_state(B& b) {
+        constexpr int n = sizeof(B) / sizeof(float);
+        float* pb = reinterpret_cast<float*>(&b);
+#pragma unroll
+        for (int i = 0; i < n; ++i) pb[i] = 0.f;
+    }
+    template <typename B>
+    static __device__ __forceinline__ void add_float(State<NC, D>& M, const B& a) {
+        constexpr int n = sizeof(B) / sizeof(float);
+        static_assert(sizeof(State<NC, D>) == n * sizeof(double), "layouts differ");
+        double* pm = reinterpret_cast<double*>(&M);
+        const float* pa = reinterpret_cast<const float*>(&a);
+#pragma unroll
+        for (int i = 0; i < n; ++i) pm[i] = pm[i] + double(pa[i]);
     }
 
     static __device__ __forceinline__ void spoil(State<NC, D>& M) {

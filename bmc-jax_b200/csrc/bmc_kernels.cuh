@@ -334,13 +334,15 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
                     }
                     g = gval;
                 }
-                StepCoef<NC, D> sc;
-                C::event_coef(cc, rec, g, sc);
+                D w1x, w1y, Rm1W;
+                C::rf_coef(cc, rec, g, w1x, w1y, Rm1W);
                 if (rec.wf != fkey) {
-                    nb = C::norm_base(sc, cc);
+                    StepCoef<NC, D> s0;
+                    C::event_coef(cc, rec, g, s0);
+                    nb = C::norm_base(s0, cc);
                     fkey = rec.wf;
                 }
-                R nu = evolve ? rec.dt * C::rf_norm(nb, sc.w1x.v, sc.w1y.v, sc.Rm1W.v) : R(0);
+                R nu = evolve ? rec.dt * C::rf_norm(nb, w1x.v, w1y.v, Rm1W.v) : R(0);
                 if (!(nu < R(INFINITY))) {                          // NaN or inf: flag, let NaN propagate
                     if (evolve) atomicOr(a.status, 1);
                     nu = R(0);
@@ -349,6 +351,8 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
                 // Taylor action with the fewest terms whose tail bound meets the tolerance
                 const bool dense_own = evolve && nu > R(tt.dense_switch);
                 if (__any_sync(kFull, dense_own)) {
+                    StepCoef<NC, D> sc;                            // unscaled: the dense path scales by dt / 2^s
+                    C::event_coef(cc, rec, g, sc);
                     if constexpr (std::is_same<R, RD>::value) {
                         Dense<NC, R, NT>::event(dsm, lane, dense_own, sc, cc, rec.dt, nu, M, tt, a.status, count, wk1, wk2);
                     } else {
@@ -383,8 +387,7 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
                 const int m_w = __reduce_max_sync(kFull, (unsigned)m_own);
                 if (ns_w > 0) {
                     const R h = tay ? (ns_own == 1 ? rec.dt : rec.dt / R(ns_own)) : R(0);
-                    C::scale_coef(sc, h);
-                    C::taylor_apply(sc, ns_w, m_w, ns_own, m_own, M, tt.inv_fact, cc, h);
+                    C::taylor_apply(cc, rec, g, h, ns_w, m_w, ns_own, m_own, M, tt);
                     if (count && tay) wk0 += unsigned(ns_own * m_own);
                     if (count) wk3 += unsigned(ns_w * m_w);
                 }
