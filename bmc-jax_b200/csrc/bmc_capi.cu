@@ -120,7 +120,7 @@ bmc_status tables(int precision, const TaylorTable** out) {
     std::lock_guard<std::mutex> lk(g_mu);
     DeviceState& ds = dev_state(dev);
     if (!ds.tables_ready) {
-        TaylorTable h[2] = {make_table(1e-13, 30, 0.5, 100.0, 1e-8),
+        TaylorTable h[2] = {make_table(1e-13, 30, 0.5, 100.0, 1e-6),
                             make_table(std::ldexp(1.0, -24), 16, 0.5, 100.0, 0.0)};
         CUDA_TRY(cudaMemcpyToSymbol(g_tables, h, sizeof(h)));
         CUDA_TRY(cudaGetSymbolAddress((void**)&ds.tables, g_tables));
@@ -884,7 +884,7 @@ bmc_status noalloc_setup(int precision, void** scratch, const TaylorTable** tt) 
         return fail(BMC_ERR_UNSUPPORTED, "bmc_simulate_noalloc: device %d above %d", dev, kNoAllocMaxDevices - 1);
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
     if (!g_noalloc_tables[dev]) {
-        TaylorTable h[2] = {make_table(1e-13, 30, 0.5, 100.0, 1e-8), make_table(std::ldexp(1.0, -24), 16, 0.5, 100.0, 0.0)};
+        TaylorTable h[2] = {make_table(1e-13, 30, 0.5, 100.0, 1e-6), make_table(std::ldexp(1.0, -24), 16, 0.5, 100.0, 0.0)};
         CUDA_TRY(cudaMemcpyToSymbol(g_tables, h, sizeof(h)));
         g_noalloc_tables[dev] = true;
     }

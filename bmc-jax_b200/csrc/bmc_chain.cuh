@@ -27,8 +27,8 @@ struct TaylorTable {
     double dense_theta;    // dense path: ||X / 2^s|| <= dense_theta ...
     int dense_m;           // ... with this Horner degree
     double dense_switch;   // warps whose largest ||X|| exceeds this take the dense path
-    // float64 kernels: for a warp of Taylor degree m, the terms from f32_from[m] on are below 1e-8 of
-    // the state (theta[m]^k / k! <= 1e-8) and are formed in float32 (> m: none)
+    // float64 kernels: for a warp of Taylor degree m, the terms from f32_from[m] on are below 1e-6 of
+    // the state (theta[m]^k / k! <= 1e-6) and are formed in float32 (> m: none)
     int f32_from[kTaylorMMax + 1];
     float inv_fact_f[kTaylorMMax + 1];  // 1 / k! in float32
 };
@@ -324,10 +324,10 @@ struct Chain {
     // The loops run to the warp's largest (s, m); each chain uses only its own (ns_own, m_own), so a
     // chain's result never depends on which chains share its warp.
     //
-    // In the float64 kernel without tangents, the terms from tt.f32_from[m_w] on (each below 1e-8 of the
+    // In the float64 kernel without tangents, the terms from tt.f32_from[m_w] on (each below 1e-6 of the
     // state, in the balanced norm of coef_norm) are formed in float32 and summed in a float32
     // accumulator that is added to M once per sub-step: their rounding, a few units of 2^-24 of terms
-    // below 1e-8, stays under 1e-14 of the state per event, below the truncation tolerance 1e-13.
+    // below 1e-6, is at most ~2e-13 of the state per event, the order of the truncation tolerance.
     static __device__ __forceinline__ void taylor_apply(const ChainConst<NC, D>& cst, const EvRec<R>& rec, D g_mt,
                                                         R h, int ns_w, int m_w, int ns_own, int m_own,
                                                         State<NC, D>& M, const TaylorTable& tt) {
