@@ -178,9 +178,9 @@ def cpu_baseline(P, M0, ev, n_cest, budget_s=15.0, kind="port"):
 
 # ------------------------------------------------------------------------------------------------
 # DRAM bytes per chain of chain_kernel from one ncu capture of a 2,048-voxel x 101-offset launch of the
-# default workload (22.3 MB read + 55.2 MB written, almost all of it register-spill traffic); it
+# default workload (22.0 MB read + 37.6 MB written, almost all of it register-spill traffic); it
 # grows with the number of chains a launch runs. Keyed by (CEST pools, precision, pulses).
-NCU_BYTES_PER_CHAIN = {(4, 0, 20): (22.317312e6 + 55.170304e6) / (2048 * 101)}
+NCU_BYTES_PER_CHAIN = {(4, 0, 20): (21.957632e6 + 37.630464e6) / (2048 * 101)}
 
 
 def run_ours(args, rank, world, local_rank):
