@@ -45,7 +45,11 @@ typedef enum {
     BMC_ERR_NUMERIC = 4,           /* a chain needed more squarings than the cap: its outputs are NaN */
 } bmc_status;
 
-/* precision of the propagation arithmetic */
+/* precision of the propagation arithmetic. BMC_F64: float64, except that in the forward model without
+ * tangents the Taylor terms below 1e-6 of the state (by the series bound) are formed in float32 and
+ * added to the float64 state once per sub-step, at most ~2e-13 of the state per event. Tangents, the
+ * dense path for long events and the LM arithmetic are float64 throughout. BMC_F32: float32 Taylor
+ * propagation, float64 dense path. */
 #define BMC_F64 0
 #define BMC_F32 1
 
