@@ -153,7 +153,7 @@ def measured_peaks():
 # ------------------------------------------------------------------------------------------------
 # CPU baseline: the C oracle on the host cores, bounded sample
 # ------------------------------------------------------------------------------------------------
-def cpu_baseline(P, M0, ev, n_cest, budget_s=15.0, kind="port"):
+def cpu_baseline(P, M0, ev, n_cest, budget_s=15.0, kind="port", return_z=False):
     sys.path.insert(0, str(ROOT / "oracle"))
     import bmc_oracle as O
     mz = 2 * (1 + n_cest)
@@ -169,11 +169,20 @@ def cpu_baseline(P, M0, ev, n_cest, budget_s=15.0, kind="port"):
     n_vox = max(1, int(budget_s / max(per_chain * n_off, 1e-9)))
     n_vox = min(n_vox, P.shape[1])
     t = time.perf_counter()
-    O.c_simulate_z(P[:, :n_vox], events, M0[:n_vox], n_cest, mz, threads)
+    z = O.c_simulate_z(P[:, :n_vox], events, M0[:n_vox], n_cest, mz, threads)
     el = time.perf_counter() - t
-    return {"value": n_vox / el, "unit": "Z-spectra/s", "cores": threads, "kind": kind,
+    line = {"value": n_vox / el, "unit": "Z-spectra/s", "cores": threads, "kind": kind,
             "sample": f"{n_vox} voxels x {n_off} offsets x {ev[0].shape[1]} events, float64 Pade-13 "
                       f"expm per event (oracle/bmc_oracle.c, OpenMP), {el:.1f} s"}
+    return (line, z) if return_z else line
+
+
+def oracle_check(P, M0, ev, n_cest, z_gpu, n_vox=8):
+    """max |dZ| of the first n_vox voxels of a timed output against the float64 C oracle (after timing)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import bmc_oracle as O
+    want = O.c_simulate_z(P[:, :n_vox], O.Events(*ev), M0[:n_vox], n_cest, 2 * (1 + n_cest))
+    return float(np.max(np.abs(np.asarray(z_gpu)[:n_vox] - want)))
 
 
 # ------------------------------------------------------------------------------------------------
@@ -264,9 +273,11 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         dist.barrier()
 
-    # end to end: host buffers in, Z back to the host, copies inside the timed region
+    # end to end: host buffers in, Z back to the host, copies inside the timed region (at most 5 steps: the
+    # copies add ~15 ms to a ~4 s step, so more steps would only lengthen the run)
     e2e = []
-    for _ in range(args.steps):
+    e2e_steps = max(1, min(args.steps, 5))
+    for _ in range(e2e_steps):
         flush.fill_(1.0)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -313,7 +324,7 @@ def run_ours(args, rank, world, local_rank):
     if (nc, prec, args.pulses) in NCU_BYTES_PER_CHAIN and not args.spread_nodes:
         traffic = NCU_BYTES_PER_CHAIN[(nc, prec, args.pulses)] * nv * n_off
         traffic_src = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one 2,048-voxel launch, scaled by "
-                       "the chains of this launch (profiles/chain_kernel_forward_2048vox.md)")
+                       "the chains of this launch")
     line = {
         "metric": "Z-spectra/s (batched forward simulation)", "value": value, "unit": "Z-spectra/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -330,7 +341,7 @@ def run_ours(args, rank, world, local_rank):
                                    "formed in float32 and summed into the float64 state once per sub-step"
                                    if prec == _lib.F64 else None)},
         "e2e": {"value": world * nv / (e2e_ms * 1e-3), "unit": "Z-spectra/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms, "steps": e2e_steps},
         "roofline": {"bound": "fp64-fma" if prec == _lib.F64 else "fp32-fma", "achieved": achieved,
                      "peak": best, "unit": "TFLOP/s", "frac": achieved / best if best else None,
                      "traffic": traffic, "traffic_unit": "bytes per launch",
@@ -342,8 +353,23 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clocks,
         "gpu_launches": 2 * args.steps,
     }
+    # the timed output itself against the float64 C oracle, on its first voxels (after timing); with the
+    # CPU baseline, on the voxels the baseline simulated
+    z_host = hZ.numpy()
     if rank == 0 and world == 1 and not args.no_cpu and not args.spread_nodes:
-        line["cpu_baseline"] = cpu_baseline(P, M0, ev, nc, budget_s=args.cpu_budget)
+        line["cpu_baseline"], z_cpu = cpu_baseline(P, M0, ev, nc, budget_s=args.cpu_budget, return_z=True)
+        n_chk = z_cpu.shape[0]
+        err = float(np.max(np.abs(z_host[:n_chk] - z_cpu)))
+    elif not args.spread_nodes:
+        n_chk = min(nv, 4)
+        err = oracle_check(P, M0, ev, nc, z_host, n_chk)
+    else:
+        n_chk, err = 0, None
+    line["config"]["oracle_check"] = {"voxels": n_chk, "offsets": n_off,
+                                      "max_abs_err_vs_float64_oracle": err,
+                                      "oracle": "oracle/bmc_oracle.c (float64 Pade-13 expm per event)"}
+    if world == 1 and not args.no_fit and not args.spread_nodes:
+        line["fit"] = warm_vs_plain(args, rank, local_rank, peak_fp64=best if prec == _lib.F64 else None)
     return line
 
 
@@ -815,13 +841,119 @@ def run_uneven(args, rank, world, local_rank):
                        "cost_first_last": [float(res.cost[0]), float(res.cost[-1])]}}
 
 
-def run_warmfit(args, rank, world, local_rank):
+def lm_tangent_roofline(exp, spec, X_phys, peak):
+    """The LM's tangent pass as the fit runs it (every free parameter's derivative at every offset, one
+    launch per tangent, the primal carried along as dual numbers) on `X_phys`, timed with CUDA events on
+    the launching stream, against the kernel's own counts of the work it executed. Dual-number FLOPs:
+    each primal multiply-add becomes 1 + 2 T (T tangents per launch), so a launch's FLOPs are its counted
+    primal FLOPs times (1 + 2 T)."""
+    import ctypes as C
+    import torch
+    from bmc_b200 import _lib
+    from bmc_b200.fitting import write_params, field_row
+    from bmc_b200.simulation import DeviceEvents, pack_params, problem, tile_params, n_cest_of, state_size
+    n = X_phys.shape[0]
+    nc = n_cest_of(exp.params)
+    N = state_size(nc)
+    P = spec.n
+    p = write_params(tile_params(exp.params, n), spec.to_scaled(X_phys), spec)
+    dev_ev = DeviceEvents(exp.events)
+    dP = torch.as_tensor(pack_params(p, n)).cuda()
+    dM = torch.as_tensor(np.broadcast_to(np.asarray(exp.m0, np.float64), (n, N)).copy()).cuda()
+    z = torch.empty((n, dev_ev.n_offsets), dtype=torch.float64, device="cuda")
+    jz = torch.empty((P, n, dev_ev.n_offsets), dtype=torch.float64, device="cuda")
+    seed = torch.as_tensor(np.tile(spec.scales[:, None], (1, n))).cuda()
+    tg = _lib.Tangents()
+    tg.n_tangents = P
+    for i, sl in enumerate(spec.slots):
+        tg.field_row[i] = field_row(sl.field, sl.index, nc)
+    tg.d_seed, tg.d_dm0 = seed.data_ptr(), None
+    pr = problem(n, dev_ev.n_offsets, dev_ev.n_events, nc, int(exp.mz_loc), _lib.F64)
+    L = _lib.lib()
+    stream = torch.cuda.current_stream()
+    sh = C.c_void_p(stream.cuda_stream)
+    call = lambda: _lib.check(L.bmc_simulate_jvp(pr, _lib.ptr(dP), dev_ev.struct, _lib.ptr(dM), None, tg,
+                                                 _lib.ptr(z), _lib.ptr(jz), sh))
+    call()
+    work = torch.zeros(4, dtype=torch.int64, device="cuda")
+    _lib.check(L.bmc_simulate_jvp_counted(pr, _lib.ptr(dP), dev_ev.struct, _lib.ptr(dM), None, tg, _lib.ptr(z),
+                                          _lib.ptr(jz), _lib.ptr(work), sh))
+    torch.cuda.synchronize()
+    terms, hcols, squar, executed = [int(x) for x in work.cpu()]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    call()
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    T = 2 if nc <= 1 else 1                                  # tangents per launch (the library's choice)
+    nnz = 12 + 15 * nc
+    flop_term = 2 * nnz + 2 * N
+    flops = (terms * flop_term + hcols * flop_term + squar * 2.0 * N * N * (N + 1)) * (1 + 2 * T)
+    tf = flops / (ms * 1e-3) / 1e12
+    return {"bound": "fp64-fma", "achieved": tf, "peak": peak, "unit": "TFLOP/s",
+            "frac": tf / peak if peak else None, "traffic": None,
+            "kernel": f"chain_kernel<{nc}, double, {T}> (LM tangent pass, {P} launches)",
+            "voxels": n, "offsets": dev_ev.n_offsets, "ms": ms, "flops": flops, "taylor_terms": terms,
+            "dense_columns": hcols, "dense_squarings": squar,
+            "peak_source": "the forward leg's FP64 FMA probe of this run (burst)"}
+
+
+def _oracle_lm_worker(job):
+    """One voxel's plain LM on the float64 oracle for `n_iter` iterations (a spawn-pool worker)."""
+    sys.path[:0] = [str(ROOT / "bmc-jax_b200"), str(ROOT / "oracle")]
+    import bmc_oracle as O
+    p, ev, m0, slots, z, x0, lo, hi, n_iter = job
+    p, ev = O.Params(*p), O.Events(*ev)
+    slots = [O.Slot(*s) for s in slots]
+    t = time.perf_counter()
+    O.fit_voxel(p, ev, m0, slots, z, x0, lo, hi, n_iter=n_iter)
+    return time.perf_counter() - t
+
+
+def fit_cpu_baseline(exp, spec, X_true, z, frac_plain, n_iter=30, sample_iters=3):
+    """Plain LM on the float64 NumPy oracle (oracle.fit_voxel: the reference's LM schedule, exact
+    forward-mode Jacobian, scipy expm per event), one voxel per host core in a spawn pool, timed for
+    `sample_iters` iterations and extrapolated to n_iter (every iteration costs the same: one Jacobian and
+    one trial residual); fitted voxels/s = cores x fraction within 1% (the GPU plain LM's, the same
+    algorithm) / seconds per voxel."""
+    import multiprocessing as mp
+    cores = max(1, min(os.cpu_count() or 1, 32, len(z)))
+    p = tuple(np.asarray(v, np.float64) for v in exp.params)
+    ev = tuple(np.asarray(a) for a in exp.events)
+    slots = [(s.field, s.index, s.scale) for s in spec.slots]
+    m0 = np.asarray(exp.m0, np.float64)
+    jobs = [(p, ev, m0, slots, z[i], spec.x0_phys, spec.lo_phys, spec.hi_phys, sample_iters) for i in range(cores)]
+    # one BLAS thread per worker process (the workers inherit the environment at spawn)
+    keys = ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS")
+    saved = {k: os.environ.get(k) for k in keys}
+    os.environ.update({k: "1" for k in keys})
+    try:
+        with mp.get_context("spawn").Pool(cores) as pool:
+            t0 = time.perf_counter()
+            secs = pool.map(_oracle_lm_worker, jobs)
+            wall = time.perf_counter() - t0
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    per_voxel = float(np.mean(secs)) * n_iter / sample_iters
+    return {"value": cores * frac_plain / per_voxel, "unit": "voxels/s", "cores": cores, "kind": "port",
+            "sample": f"{cores} voxels (one per process), {sample_iters} of {n_iter} plain LM iterations each "
+                      f"({float(np.mean(secs)):.1f} s, {wall:.1f} s wall), float64 NumPy oracle "
+                      f"(oracle/bmc_oracle.py fit_voxel); extrapolated to {n_iter} iterations and scaled by the "
+                      f"fraction within 1% ({frac_plain:.3f})"}
+
+
+def warm_vs_plain(args, rank, local_rank, peak_fp64=None):
     """Fitted voxels/s at <=1% parameter error, NN-warm vs plain LM: train the warm-start network on
-    `--train` simulated ladders (noise sigma 0.005), then fit `--voxels` held-out noise-free voxels
+    `--train` simulated ladders (noise sigma 0.005), then fit `--fit-voxels` held-out noise-free voxels
     (a) plainly, 30 iterations from the fixed x0, and (b) from the network's x0 with `--warm-iters`
-    iterations plus the plain refit of every voxel whose rms ends above 1e-4. Both timed end to end
-    through the public API (fitting.fit, LadderWarmStart.fit), host buffers in and out."""
-    import time
+    iterations plus the plain refit of every voxel whose warm fit ends above the rms threshold (keeping
+    the better of the two). Both timed end to end through the public API (fitting.fit,
+    LadderWarmStart.fit), host buffers in and out."""
     import torch
     from bmc_b200.fitting import fit
     from bmc_b200.warmstart import LadderWarmStart
@@ -842,7 +974,7 @@ def run_warmfit(args, rank, world, local_rank):
     del Z, T
     torch.cuda.empty_cache()
 
-    n = args.voxels
+    n = args.fit_voxels
     X_true = ws.draw(n, seed + 7919)
     z = ws.simulate64(X_true)
     # warm-up of both paths on a small slice (library load, workspaces, kernel attributes)
@@ -858,26 +990,63 @@ def run_warmfit(args, rank, world, local_rank):
     ok_p = within_1pct(plain.x, X_true, names)
     ok_w = within_1pct(warm.x, X_true, names)
     x0_err = np.median(np.abs(warm.x0 / X_true - 1.0), axis=0)
-    roof = mlp_roofline(ws.n_points, spec.n)
-    v_w = world * ok_w.sum() / warm_s
-    v_p = world * ok_p.sum() / plain_s
-    return {"metric": "fitted voxels/s at <=1% param err, NN-warm vs plain LM", "value": v_w, "unit": "voxels/s",
-            "n_gpus": world, "steps": 1, "warmup": 1, "ms_per_step": warm_s * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64 LM, bf16/fp32 MLP",
+    v_w = ok_w.sum() / warm_s
+    v_p = ok_p.sum() / plain_s
+    out = {"workload": f"warm-started LM: {n} voxels, water + {args.pools} CEST pools"
+                       f"{' + MT' if args.pools >= 3 else ''}, ladder 4 x 61 CW (2 s), "
+                       f"{spec.n} free ({', '.join(names)}); noise-free held-out voxels, parameters uniform in "
+                       "the training ranges",
+           "warm_fitted_voxels_per_s": v_w, "plain_fitted_voxels_per_s": v_p,
+           "warm_over_plain": v_w / v_p if v_p else None, "unit": "voxels/s",
+           "fraction_within_1pct": {"warm": float(ok_w.mean()), "plain": float(ok_p.mean())},
+           "within_1pct_rule": "every free parameter within 1% of its truth (the B0 shift within 0.003 ppm)",
+           "seconds": {"plain_lm": plain_s, "warm_total": warm_s,
+                       **{f"warm_{k}": v for k, v in warm.seconds.items()}},
+           "warm_iters": args.warm_iters, "plain_iters": 30, "refit_fraction": float(warm.refit.mean()),
+           "median_x0_rel_err": dict(zip(names, map(float, x0_err))),
+           "training": {"spectra": args.train, "epochs": args.epochs, "batch": 4096, "lr": 1e-3,
+                        "simulate_s": gen_s, "train_s": train_s, "loss_first_last": [hist[0], hist[-1]],
+                        "noise_sigma": 0.005},
+           "mlp_roofline": mlp_roofline(ws.n_points, spec.n)}
+    if peak_fp64 is None:
+        peak_fp64 = fp64_peak()
+    out["roofline"] = lm_tangent_roofline(exp, spec, X_true, peak_fp64)
+    if not args.no_cpu:
+        out["cpu_baseline"] = fit_cpu_baseline(exp, spec, X_true, z, float(ok_p.mean()))
+    return out
+
+
+def fp64_peak():
+    """FP64 FMA throughput of this GPU now (TFLOP/s, best of three probe launches)."""
+    import ctypes as C
+    import torch
+    from bmc_b200 import _lib
+    stream = torch.cuda.current_stream()
+    fl = C.c_double(0.0)
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    best = 0.0
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _lib.check(_lib.lib().bmc_probe_fma_peak(_lib.F64, sms * 8, 4096, C.byref(fl),
+                                                 C.c_void_p(stream.cuda_stream)))
+        e1.record(stream)
+        e1.synchronize()
+        best = max(best, fl.value / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    return best
+
+
+def run_warmfit(args, rank, world, local_rank):
+    """The warm-vs-plain fit (warm_vs_plain) as its own bench line."""
+    r = warm_vs_plain(args, rank, local_rank)
+    return {"metric": "fitted voxels/s at <=1% param err, NN-warm vs plain LM", "value": world * r["warm_fitted_voxels_per_s"],
+            "unit": "voxels/s", "n_gpus": world, "steps": 1, "warmup": 1,
+            "ms_per_step": r["seconds"]["warm_total"] * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 LM, bf16/fp32 MLP",
             "data": "synthetic (seeded): parameters uniform in the ranges, noise-free held-out voxels",
-            "config": {"workload": f"warm-started LM: {n} voxels, water + {args.pools} CEST pools"
-                                   f"{' + MT' if args.pools >= 3 else ''}, ladder 4 x 61 CW (2 s), "
-                                   f"{spec.n} free ({', '.join(names)})",
-                       "plain_voxels_per_s": v_p, "speedup_vs_plain": v_w / v_p if v_p else None,
-                       "fraction_within_1pct": {"warm": float(ok_w.mean()), "plain": float(ok_p.mean())},
-                       "seconds": {"plain_lm": plain_s, "warm_total": warm_s,
-                                   **{f"warm_{k}": v for k, v in warm.seconds.items()}},
-                       "warm_iters": args.warm_iters, "plain_iters": 30, "refit_fraction": float(warm.refit.mean()),
-                       "median_x0_rel_err": dict(zip(names, map(float, x0_err))),
-                       "training": {"spectra": args.train, "epochs": args.epochs, "batch": 4096, "lr": 1e-3,
-                                    "simulate_s": gen_s, "train_s": train_s, "loss_first_last": [hist[0], hist[-1]],
-                                    "noise_sigma": 0.005}},
-            "roofline": roof}
+            "config": {k: v for k, v in r.items() if k not in ("roofline", "cpu_baseline", "mlp_roofline")},
+            "roofline": r["roofline"], "mlp_roofline": r["mlp_roofline"],
+            **({"cpu_baseline": r["cpu_baseline"]} if "cpu_baseline" in r else {})}
 
 
 def main():
@@ -894,6 +1063,8 @@ def main():
     ap.add_argument("--warm-iters", type=int, default=8, help="warmfit: LM iterations from the network's x0")
     ap.add_argument("--spread-nodes", type=int, default=0, help="forward: B0-spread isochromats per voxel")
     ap.add_argument("--voxels", type=int, default=65536)
+    ap.add_argument("--fit-voxels", type=int, default=65536, help="warm-vs-plain fit: held-out voxels")
+    ap.add_argument("--no-fit", action="store_true", help="forward: leave out the warm-vs-plain fit leg")
     ap.add_argument("--offsets", type=int, default=101)
     ap.add_argument("--pulses", type=int, default=20)
     ap.add_argument("--pools", type=int, default=4, choices=[1, 2, 3, 4, 5])

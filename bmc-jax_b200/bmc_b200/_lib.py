@@ -24,8 +24,8 @@ SLOT_SPREAD_SIGMA, SLOT_M_START = -2, -3
 
 EXPORTS = ("bmc_abi_version", "bmc_version", "bmc_last_error", "bmc_release", "bmc_simulate",
            "bmc_simulate_jvp", "bmc_simulate_trajectory", "bmc_lm_fit", "bmc_normal_blocks",
-           "bmc_simulate_counted", "bmc_probe_fma_peak", "bmc_simulate_noalloc", "bmc_mlp_sizes", "bmc_mlp_sync",
-           "bmc_mlp_forward", "bmc_mlp_backward", "bmc_mlp_adam_step", "bmc_uneven_create", "bmc_uneven_simulate",
+           "bmc_simulate_counted", "bmc_simulate_jvp_counted", "bmc_probe_fma_peak", "bmc_simulate_noalloc",
+           "bmc_mlp_sizes", "bmc_mlp_sync", "bmc_mlp_forward", "bmc_mlp_backward", "bmc_mlp_adam_step", "bmc_uneven_create", "bmc_uneven_simulate",
            "bmc_uneven_destroy", "bmc_normal_segments", "bmc_schur_step", "bmc_schur_eliminate", "bmc_schur_back")
 
 
@@ -99,6 +99,9 @@ def lib():
         L.bmc_simulate_counted.argtypes = [C.POINTER(Problem), vp, C.POINTER(Events), vp, C.POINTER(Spread), vp,
                                            vp, vp]
         L.bmc_simulate_counted.restype = C.c_int
+        L.bmc_simulate_jvp_counted.argtypes = [C.POINTER(Problem), vp, C.POINTER(Events), vp, C.POINTER(Spread),
+                                               C.POINTER(Tangents), vp, vp, vp, vp]
+        L.bmc_simulate_jvp_counted.restype = C.c_int
         L.bmc_probe_fma_peak.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double), vp]
         L.bmc_probe_fma_peak.restype = C.c_int
         L.bmc_simulate_noalloc.argtypes = [C.POINTER(Problem), vp, C.POINTER(Events), vp, C.POINTER(Spread), vp, vp]

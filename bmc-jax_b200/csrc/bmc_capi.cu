@@ -7,10 +7,12 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -103,11 +105,17 @@ __device__ TaylorTable g_tables[2];   // [BMC_F64, BMC_F32], per device
 struct DeviceState {
     bool tables_ready = false;
     TaylorTable* tables = nullptr;   // device address of g_tables, taken once
-    void* ws = nullptr;
-    size_t ws_bytes = 0;
 };
 std::mutex g_mu;
 std::vector<DeviceState> g_dev;
+
+// Workspaces, one per (device, stream): calls on different streams never share scratch, so they may run
+// concurrently from different host threads; calls on one stream are ordered by the stream itself.
+struct Workspace {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+std::map<std::pair<int, cudaStream_t>, Workspace> g_ws;
 
 DeviceState& dev_state(int dev) {
     if ((int)g_dev.size() <= dev) g_dev.resize(dev + 1);
@@ -130,24 +138,32 @@ bmc_status tables(int precision, const TaylorTable** out) {
     return BMC_OK;
 }
 
-// one cached workspace per device, grown on demand (the caller serialises calls that share it)
-bmc_status workspace(size_t bytes, void** out) {
+// The cached workspace of the current device and `st`, grown on demand in stream order: the old buffer
+// is released by cudaFreeAsync on the same stream (after the work already queued there that uses it) and
+// the new one taken by cudaMallocAsync, so growing never synchronises the device. A call that grows the
+// workspace allocates (it is not capturable in a CUDA graph); later calls of the same or a smaller size
+// only enqueue kernels.
+bmc_status workspace(size_t bytes, cudaStream_t st, void** out) {
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
     std::lock_guard<std::mutex> lk(g_mu);
-    DeviceState& ds = dev_state(dev);
-    if (ds.ws_bytes < bytes) {
-        if (ds.ws) {
-            CUDA_TRY(cudaDeviceSynchronize());
-            CUDA_TRY(cudaFree(ds.ws));
-            ds.ws = nullptr;
-            ds.ws_bytes = 0;
+    Workspace& w = g_ws[{dev, st}];
+    if (w.bytes < bytes) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        CUDA_TRY(cudaStreamIsCapturing(st, &cs));
+        if (cs != cudaStreamCaptureStatusNone)
+            return fail(BMC_ERR_INVALID, "this call needs %zu workspace bytes on a stream that is being captured and "
+                        "has %zu: make one call of this size on the same stream before capturing", bytes, w.bytes);
+        if (w.ptr) {
+            CUDA_TRY(cudaFreeAsync(w.ptr, st));
+            w.ptr = nullptr;
+            w.bytes = 0;
         }
         const size_t want = bytes + bytes / 4 + (1 << 20);
-        CUDA_TRY(cudaMalloc(&ds.ws, want));
-        ds.ws_bytes = want;
+        CUDA_TRY(cudaMallocAsync(&w.ptr, want, st));
+        w.bytes = want;
     }
-    *out = ds.ws;
+    *out = w.ptr;
     return BMC_OK;
 }
 
@@ -239,14 +255,14 @@ bmc_status launch_chain(const ChainArgs& a, const TaylorTable* tt, cudaStream_t 
     const size_t smem = kWarps * sizeof(DenseSmem<NC, typename DenseReal<R>::type, NT>) +
                         32 * kWarps * sizeof(ChainConst<NC, Dn<R, NT>>);
     // the attribute once per device and instantiation: later calls then only enqueue work (which keeps
-    // them capturable in a CUDA graph)
-    static unsigned long long configured = 0;
+    // them capturable in a CUDA graph). Atomic: calls on several devices may come from several threads.
+    static std::atomic<unsigned long long> configured{0};
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
-    if (dev >= 64 || !((configured >> dev) & 1ull)) {
+    if (dev >= 64 || !((configured.load(std::memory_order_acquire) >> dev) & 1ull)) {
         CUDA_TRY(cudaFuncSetAttribute(chain_kernel<NC, R, NT, U>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
-        if (dev < 64) configured |= 1ull << dev;
+        if (dev < 64) configured.fetch_or(1ull << dev, std::memory_order_acq_rel);
     }
     const long long nch = U ? a.n_chains : (long long)a.n_vox * a.n_off;
     const long long blocks = (nch + 127) / 128;
@@ -369,7 +385,7 @@ struct Impl {
         void* ws = nullptr;
         const size_t recb = pr->precision == BMC_F32 ? sizeof(EvRec<float>) : sizeof(EvRec<double>);
         const long long nch = (long long)pr->n_voxels * pr->n_offsets;
-        if ((s = workspace(align256(nrec * recb) + 256 + order_bytes(nch), &ws)) != BMC_OK) return s;
+        if ((s = workspace(align256(nrec * recb) + 256 + order_bytes(nch), st, &ws)) != BMC_OK) return s;
         Carve cv(ws);
         ChainArgs a{};
         a.n_vox = pr->n_voxels; a.n_off = pr->n_offsets; a.n_ev = pr->n_events; a.n_fields = Layout<NC>::NF;
@@ -399,7 +415,7 @@ struct Impl {
         if (s != BMC_OK) return s;
         const size_t nrec = (size_t)pr->n_offsets * pr->n_events;
         void* ws = nullptr;
-        if ((s = workspace(align256(nrec * sizeof(EvRec<double>)) + 256 + align256(sizeof(double) * pr->n_voxels * pr->n_offsets), &ws)) != BMC_OK) return s;
+        if ((s = workspace(align256(nrec * sizeof(EvRec<double>)) + 256 + align256(sizeof(double) * pr->n_voxels * pr->n_offsets), st, &ws)) != BMC_OK) return s;
         Carve cv(ws);
         ChainArgs a{};
         a.n_vox = pr->n_voxels; a.n_off = pr->n_offsets; a.n_ev = pr->n_events; a.n_fields = Layout<NC>::NF;
@@ -416,20 +432,21 @@ struct Impl {
     }
 
     static bmc_status jvp(const bmc_problem* pr, const double* params, const bmc_events* ev, const double* m0,
-                          const bmc_spread* sp, const bmc_tangents* tg, double* z, double* jz, cudaStream_t st) {
+                          const bmc_spread* sp, const bmc_tangents* tg, double* z, double* jz, cudaStream_t st,
+                          unsigned long long* work = nullptr) {
         const TaylorTable* tt = nullptr;
         bmc_status s = tables(BMC_F64, &tt);
         if (s != BMC_OK) return s;
         const size_t nrec = (size_t)pr->n_offsets * pr->n_events;
         void* ws = nullptr;
         const long long nch = (long long)pr->n_voxels * pr->n_offsets;
-        if ((s = workspace(align256(nrec * sizeof(EvRec<double>)) + 256 + order_bytes(nch), &ws)) != BMC_OK) return s;
+        if ((s = workspace(align256(nrec * sizeof(EvRec<double>)) + 256 + order_bytes(nch), st, &ws)) != BMC_OK) return s;
         Carve cv(ws);
         ChainArgs a{};
         a.n_vox = pr->n_voxels; a.n_off = pr->n_offsets; a.n_ev = pr->n_events; a.n_fields = Layout<NC>::NF;
         a.mz = pr->mz_loc; a.reset_after_adc = pr->reset_after_adc;
         if ((s = fill_spread(a, sp)) != BMC_OK) return s;
-        a.params = params; a.m0 = m0; a.out = z; a.jout = jz;
+        a.params = params; a.m0 = m0; a.out = z; a.jout = jz; a.work = work;
         for (int t = 0; t < tg->n_tangents; ++t) a.field_row[t] = tg->field_row[t];
         a.seed = tg->d_seed; a.dm0 = tg->d_dm0;
         a.status = cv.take<int>(1);
@@ -457,7 +474,7 @@ struct Impl {
                              2 * align256(sizeof(double) * nv * P) + 2 * align256(sizeof(double) * nv) +
                              align256(sizeof(int) * nv) + 4096 + order_bytes((long long)nv * no);
         void* ws = nullptr;
-        if ((s = workspace(bytes, &ws)) != BMC_OK) return s;
+        if ((s = workspace(bytes, st, &ws)) != BMC_OK) return s;
         Carve cv(ws);
         EvRec<double>* rec = cv.take<EvRec<double>>(nrec);
         double* px = cv.take<double>((size_t)NF * nv);
@@ -566,16 +583,22 @@ bmc_status bmc_release(void) {
     std::lock_guard<std::mutex> lk(g_mu);
     int cur = 0;
     cudaGetDevice(&cur);
-    for (size_t d = 0; d < g_dev.size(); ++d) {
-        if (g_dev[d].ws) {
-            cudaSetDevice((int)d);
-            cudaDeviceSynchronize();
-            cudaFree(g_dev[d].ws);
-            g_dev[d].ws = nullptr;
-            g_dev[d].ws_bytes = 0;
-        }
+    cudaError_t first = cudaSuccess;
+    for (auto& kv : g_ws) {
+        if (!kv.second.ptr) continue;
+        cudaSetDevice(kv.first.first);
+        const cudaError_t e = cudaFreeAsync(kv.second.ptr, kv.first.second);
+        if (first == cudaSuccess) first = e;
     }
+    for (auto& kv : g_ws) {
+        if (!kv.second.ptr) continue;
+        cudaSetDevice(kv.first.first);
+        const cudaError_t e = cudaStreamSynchronize(kv.first.second);
+        if (first == cudaSuccess) first = e;
+    }
+    g_ws.clear();
     cudaSetDevice(cur);
+    if (first != cudaSuccess) return fail(BMC_ERR_CUDA, "bmc_release: %s", cudaGetErrorString(first));
     return BMC_OK;
 }
 
@@ -602,6 +625,34 @@ bmc_status bmc_simulate_trajectory(const bmc_problem* prob, const double* d_para
     if (s != BMC_OK) return s;
     if (!d_traj) return fail(BMC_ERR_INVALID, "null output");
     BMC_DISPATCH(prob->n_cest, trajectory(prob, d_params, ev, d_m0, d_traj, (cudaStream_t)stream));
+}
+
+namespace {
+bmc_status check_jvp(const bmc_problem* prob, const double* d_params, const bmc_events* ev, const double* d_m0,
+                     const bmc_tangents* tan, const double* d_z, const double* d_jz) {
+    bmc_status s = check_problem(prob, d_params, ev, d_m0);
+    if (s != BMC_OK) return s;
+    if (!tan || tan->n_tangents < 1 || tan->n_tangents > BMC_MAX_TANGENTS)
+        return fail(BMC_ERR_INVALID, "tangents: 1..%d required", BMC_MAX_TANGENTS);
+    if (!tan->d_seed) return fail(BMC_ERR_INVALID, "tangents: null seed array");
+    if (prob->mz_loc < 0) return fail(BMC_ERR_INVALID, "bmc_simulate_jvp needs mz_loc >= 0");
+    if (prob->precision != BMC_F64) return fail(BMC_ERR_UNSUPPORTED, "tangents are computed in float64 only");
+    if (!d_z || !d_jz) return fail(BMC_ERR_INVALID, "null output");
+    const int nf = BMC_N_FIELDS(prob->n_cest);
+    for (int t = 0; t < tan->n_tangents; ++t)
+        if (tan->field_row[t] >= nf || tan->field_row[t] < BMC_SEED_SPREAD_SIGMA)
+            return fail(BMC_ERR_INVALID, "tangent %d: field row %d outside -2..%d", t, tan->field_row[t], nf - 1);
+    return BMC_OK;
+}
+}  // namespace
+
+bmc_status bmc_simulate_jvp_counted(const bmc_problem* prob, const double* d_params, const bmc_events* ev,
+                                    const double* d_m0, const bmc_spread* spread, const bmc_tangents* tan,
+                                    double* d_z, double* d_jz, unsigned long long* d_work, void* stream) {
+    bmc_status s = check_jvp(prob, d_params, ev, d_m0, tan, d_z, d_jz);
+    if (s != BMC_OK) return s;
+    if (!d_work) return fail(BMC_ERR_INVALID, "null counters");
+    BMC_DISPATCH(prob->n_cest, jvp(prob, d_params, ev, d_m0, spread, tan, d_z, d_jz, (cudaStream_t)stream, d_work));
 }
 
 bmc_status bmc_simulate_jvp(const bmc_problem* prob, const double* d_params, const bmc_events* ev,
@@ -861,7 +912,10 @@ bmc_status bmc_probe_fma_peak(int32_t precision, int32_t blocks, int32_t iters, 
 // scratch -- the preprocessed event records and a status word -- from one static device array,
 // g_noalloc_scratch, of kNoAllocScratchBytes on every GPU that loads the library (held until the
 // process exits). The chains run in launch order (no cost sort, which would need more scratch); the
-// results are bit-identical to bmc_simulate's, whose chains each choose their own Taylor order.
+// results are bit-identical to bmc_simulate's, since every chain chooses its own Taylor degree, sub-steps
+// and float32 switch point whatever chains share its warp. The array is reserved by the driver when it
+// loads this library's device code on a device (under lazy loading: the first bmc_* call there), so a
+// caller whose framework reserves the GPU up front makes a first call before that (or loads eagerly).
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;     // 32 MiB per GPU

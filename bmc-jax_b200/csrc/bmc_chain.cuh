@@ -324,56 +324,71 @@ struct Chain {
     // The loops run to the warp's largest (s, m); each chain uses only its own (ns_own, m_own), so a
     // chain's result never depends on which chains share its warp.
     //
-    // In the float64 kernel without tangents, the terms from tt.f32_from[m_w] on (each below 1e-6 of the
-    // state, in the balanced norm of coef_norm) are formed in float32 and summed in a float32
+    // In the float64 kernel without tangents, the terms of a chain from tt.f32_from[m_own] on (each below
+    // 1e-6 of the state, in the balanced norm of coef_norm) are formed in float32 and summed in a float32
     // accumulator that is added to M once per sub-step: their rounding, a few units of 2^-24 of terms
     // below 1e-6, is at most ~2e-13 of the state per event, the order of the truncation tolerance.
-    static __device__ __forceinline__ void taylor_apply(const ChainConst<NC, D>& cst, const EvRec<R>& rec, D g_mt,
-                                                        R h, int ns_w, int m_w, int ns_own, int m_own,
-                                                        State<NC, D>& M, const TaylorTable& tt) {
+    // The switch point is the chain's own: where the lanes of a warp disagree on it, the sub-step runs
+    // once per distinct switch point, each lane adding its terms only in its own pass (weight 0 in the
+    // others), so the result stays independent of the chains that share the warp. Cost-sorted warps
+    // almost always agree (one pass). Returns the number of passes over all sub-steps.
+    static __device__ __forceinline__ int taylor_apply(const ChainConst<NC, D>& cst, const EvRec<R>& rec, D g_mt,
+                                                       R h, int ns_w, int m_w, int ns_own, int m_own,
+                                                       State<NC, D>& M, const TaylorTable& tt) {
         constexpr bool kMixed = std::is_same<R, double>::value && NT == 0;
         // The terms are added to M as they are formed (later terms derive from `term`, not from M), so no
         // separate accumulator is held; a lane past its own sub-steps or degree adds with weight 0.
         // fma(1, t, M) rounds like M + t and fma(0, t, M) is M: the result is that of summing apart.
-        const int k32 = kMixed ? tt.f32_from[m_w] : m_w + 1;
+        int passes = 0;
 #pragma unroll 1
         for (int j = 0; j < ns_w; ++j) {
             const bool on = j < ns_own;
-            const int m_on = on ? m_own : 0;
-            StepCoef<NC, D> s;
-            event_coef(cst, rec, g_mt, s);
-            scale_coef(s, h);
-            State<NC, D> term;
-            matvec<true>(s, M, term, &cst, h);
-            fma_state(M, on ? R(1) : R(0), term);
-            int k = 2;
+            // this lane's switch point (0: no sub-step of its own here); lanes still to be served
+            const int k32_own = on ? (kMixed ? tt.f32_from[m_own] : m_w + 1) : 0;
+            unsigned pend = __ballot_sync(0xffffffffu, k32_own != 0);
 #pragma unroll 1
-            for (; k <= m_w && k < k32; ++k) {
-                State<NC, D> nt;
-                matvec<false>(s, term, nt);
-                term = nt;
-                fma_state(M, k <= m_on ? R(tt.inv_fact[k]) : R(0), term);
-            }
-            if constexpr (kMixed) {
-                if (k <= m_w) {
-                    using C32 = Chain<NC, float, 0>;
-                    using F = Dn<float, 0>;
-                    StepCoef<NC, F> s32;
-                    State<NC, F> t32, a32;
-                    to_float(s, s32);
-                    to_float(term, t32);
-                    zero_state(a32);
+            do {
+                const int k32 = __shfl_sync(0xffffffffu, k32_own, __ffs(pend) - 1);
+                const bool member = k32_own == k32;
+                pend &= ~__ballot_sync(0xffffffffu, member);
+                ++passes;
+                const int m_on = member ? m_own : 0;
+                StepCoef<NC, D> s;
+                event_coef(cst, rec, g_mt, s);
+                scale_coef(s, h);
+                State<NC, D> term;
+                matvec<true>(s, M, term, &cst, h);
+                fma_state(M, member ? R(1) : R(0), term);
+                int k = 2;
 #pragma unroll 1
-                    for (; k <= m_w; ++k) {
-                        State<NC, F> n32;
-                        C32::template matvec<false>(s32, t32, n32);
-                        t32 = n32;
-                        C32::fma_state(a32, k <= m_on ? tt.inv_fact_f[k] : 0.f, t32);
-                    }
-                    add_float(M, a32);
+                for (; k <= m_w && k < k32; ++k) {
+                    State<NC, D> nt;
+                    matvec<false>(s, term, nt);
+                    term = nt;
+                    fma_state(M, k <= m_on ? R(tt.inv_fact[k]) : R(0), term);
                 }
-            }
+                if constexpr (kMixed) {
+                    if (k <= m_w) {
+                        using C32 = Chain<NC, float, 0>;
+                        using F = Dn<float, 0>;
+                        StepCoef<NC, F> s32;
+                        State<NC, F> t32, a32;
+                        to_float(s, s32);
+                        to_float(term, t32);
+                        zero_state(a32);
+#pragma unroll 1
+                        for (; k <= m_w; ++k) {
+                            State<NC, F> n32;
+                            C32::template matvec<false>(s32, t32, n32);
+                            t32 = n32;
+                            C32::fma_state(a32, k <= m_on ? tt.inv_fact_f[k] : 0.f, t32);
+                        }
+                        add_float(M, a32);
+                    }
+                }
+            } while (pend);
         }
+        return passes;
     }
 
     // elementwise precision changes between structs made only of Dn<., 0> members (StepCoef, State)

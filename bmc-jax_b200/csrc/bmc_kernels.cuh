@@ -129,12 +129,14 @@ struct Dense {
                 if (c == lane) my_slot = g;
                 if (g == grp) grp_owner = c;
             }
+            bool capped = false;   // more squarings needed than the cap: this chain's state becomes NaN
             if (my_slot >= 0) {
                 SL* sl = &sm->slot[my_slot];
                 int s = 0;
                 if (nu > R(tt.dense_theta)) s = (int)ceil(log2(double(nu) / tt.dense_theta));
                 if (s > 200) {
                     s = 200;
+                    capped = true;
                     atomicOr(status, 2);
                 }
                 StepCoef<NC, D> scs = sc;
@@ -214,7 +216,8 @@ struct Dense {
             __syncwarp();
             if (my_slot >= 0) {
 #pragma unroll
-                for (int q = 0; q < N; ++q) C::at(M, q) = sm->slot[my_slot].out[q];
+                for (int q = 0; q < N; ++q)
+                    C::at(M, q) = capped ? dconst<R, NT>(R(NAN)) : sm->slot[my_slot].out[q];
             }
             __syncwarp();
         }
@@ -387,9 +390,9 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
                 const int m_w = __reduce_max_sync(kFull, (unsigned)m_own);
                 if (ns_w > 0) {
                     const R h = tay ? (ns_own == 1 ? rec.dt : rec.dt / R(ns_own)) : R(0);
-                    C::taylor_apply(cc, rec, g, h, ns_w, m_w, ns_own, m_own, M, tt);
+                    const int passes = C::taylor_apply(cc, rec, g, h, ns_w, m_w, ns_own, m_own, M, tt);
                     if (count && tay) wk0 += unsigned(ns_own * m_own);
-                    if (count) wk3 += unsigned(ns_w * m_w);
+                    if (count) wk3 += unsigned(passes * m_w);
                 }
             }
             if (type == EV_GRADIENT || type == EV_SPOILER) C::spoil(M);

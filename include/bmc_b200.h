@@ -42,8 +42,13 @@ typedef enum {
     BMC_ERR_INVALID = 1,           /* a size, pointer or option is out of range */
     BMC_ERR_CUDA = 2,              /* a CUDA runtime call failed */
     BMC_ERR_UNSUPPORTED = 3,       /* e.g. n_cest above BMC_MAX_CEST */
-    BMC_ERR_NUMERIC = 4,           /* a chain needed more squarings than the cap: its outputs are NaN */
+    BMC_ERR_NUMERIC = 4,           /* reserved; see "Numerical failures" below */
 } bmc_status;
+
+/* Numerical failures. The calls are asynchronous, so a failure found while the kernels run cannot be
+ * returned as a status: a chain whose generator has a non-finite norm, or that would need more
+ * squarings than the cap of 200, carries NaN to its outputs (Z, tangents, fitted values), as the
+ * reference's NaN propagates. Callers test the outputs with isfinite. */
 
 /* precision of the propagation arithmetic. BMC_F64: float64, except that in the forward model without
  * tangents the Taylor terms below 1e-6 of the state (by the series bound) are formed in float32 and
@@ -182,13 +187,19 @@ bmc_status bmc_normal_blocks(int32_t n_voxels, int32_t n_points, int32_t n_tange
  * callers that cannot let a library call cudaMalloc -- a handler inside JAX/XLA (JAX reserves most of
  * the GPU's memory for its own allocator), code under another framework's fixed memory budget, or a
  * latency-bound pipeline (cudaMalloc/cudaFree synchronise the device). Same arguments and results as
- * bmc_simulate (bit-identical Z). Its only scratch, the preprocessed event records and a status word,
- * lives in one static device array of 32 MiB per GPU that loads the library, held until exit, so
- * n_offsets x n_events may be at most 699,045 records in float64 (1,048,568 in float32); larger tables
- * are rejected with BMC_ERR_INVALID and a message. The first call on a device takes the array's
- * device address and uploads the Taylor tables (issue it before any stream capture). Every call reuses
- * the same array and overwrites the previous call's records: calls that overlap on the GPU (other
- * streams, other host threads) race and must be serialised by the caller.
+ * bmc_simulate (bit-identical Z: every chain chooses its own Taylor degree and float32 switch point, so
+ * the order the chains run in does not matter). Its only scratch, the preprocessed event records and a
+ * status word, lives in one static device array of 32 MiB per GPU that loads the library, held until
+ * exit, so n_offsets x n_events may be at most 699,045 records in float64 (1,048,568 in float32);
+ * larger tables are rejected with BMC_ERR_INVALID and a message. The CUDA driver reserves the array
+ * when it loads the library's device code on a device, which under CUDA's default lazy loading is the
+ * first bmc_* call there: a caller whose framework reserves most of the GPU up front (JAX's
+ * preallocation) makes one call, e.g. a bmc_simulate_noalloc of a tiny problem, on every device before
+ * that reservation, or runs with CUDA_MODULE_LOADING=EAGER. The first call on a device also takes the
+ * array's device address and uploads the Taylor tables (issue it before any stream capture). Every call
+ * reuses the same array and overwrites the previous call's records: calls that overlap on the GPU
+ * (other streams, other host threads) race and must be serialised by the caller. Numerical failures
+ * show as NaN in d_out, as for bmc_simulate; the status word is not reported.
  */
 bmc_status bmc_simulate_noalloc(const bmc_problem* prob, const double* d_params, const bmc_events* ev,
                                 const double* d_m0, const bmc_spread* spread, double* d_out, void* stream);
@@ -298,12 +309,18 @@ bmc_status bmc_mlp_adam_step(const bmc_mlp_shape* shape, float* d_params, const 
  *   zeroed by the caller): [0] Taylor sub-step terms each chain needed (one sparse operator product
  *   each), [1] dense-path Horner column products, [2] dense-path squarings, [3] Taylor terms executed
  *   (a warp runs to the largest need among its chains).
+ * bmc_simulate_jvp_counted: bmc_simulate_jvp that adds the same four counts to d_work[4], summed over
+ *   its launches: one per tangent (two per launch for at most one CEST pool), each carrying the primal
+ *   and its tangents through the same steps as dual numbers.
  * bmc_probe_fma_peak: launches `blocks` x 256 threads of 8 independent FMA chains x `iters`
  *   (float64 or float32) and returns the FLOPs one launch executes, to time against.
  */
 bmc_status bmc_simulate_counted(const bmc_problem* prob, const double* d_params, const bmc_events* ev,
                                 const double* d_m0, const bmc_spread* spread, double* d_out,
                                 unsigned long long* d_work, void* stream);
+bmc_status bmc_simulate_jvp_counted(const bmc_problem* prob, const double* d_params, const bmc_events* ev,
+                                    const double* d_m0, const bmc_spread* spread, const bmc_tangents* tan,
+                                    double* d_z, double* d_jz, unsigned long long* d_work, void* stream);
 bmc_status bmc_probe_fma_peak(int32_t precision, int32_t blocks, int32_t iters, double* flops_per_launch,
                               void* stream);
 

@@ -1,9 +1,10 @@
 """The CUDA path against the reference's golden vectors and the float64 oracle.
 
 Tolerances: float64 propagation agrees with the reference's float64 path to ~1e-12; the tests hold it
-to 1e-10 absolute in Z (the target for this path is 1e-5). The float32 kernel is held to 1e-5 on
-the CW ladder (the reference's own float32 path is ~1e-4 off). Jacobians: 1e-8 relative against the
-oracle's exact forward mode, 1e-4 against the reference's central differences.
+to 1e-10 absolute in Z (the target for this path is 1e-5). The all-float32 kernel (BMC_F32) is held to
+1e-4, the reference's own float32 level (settings.py:10-11); it does not meet 1e-5 on long pulse
+trains. Jacobians: 1e-8 relative against the oracle's exact forward mode, 1e-4 against the reference's
+central differences.
 """
 import numpy as np
 import pytest
@@ -151,6 +152,30 @@ def test_padding_is_a_bit_exact_no_op_and_stacking_reproduces_blocks(cuda):
     zj = joint.simulate()
     for i, part in enumerate(parts):
         assert np.abs(zj[i * 21:(i + 1) * 21] - part.simulate()).max() == 0.0
+
+
+def test_stacking_is_bit_exact_with_mixed_taylor_degrees(cuda):
+    """Stacking on pulsed trains, whose 0.25-1.25 ms samples take the Taylor path with a degree that
+    changes across the offsets (and with B1): a stacked chain shares its warp with other chains than it
+    does alone, so each chain's float64/float32 split and degree must be its own. Compared with ==."""
+    from bmc_b200.fitting import Experiment
+    from bmc_b200.simulation import SimParams, SimEvent, pad_events
+    pb = _random_batch(1, 2, seed=3, mt=True)
+    p1 = SimParams(*O.sample(pb, 0))
+    m0 = O.initial_state(O.sample(pb, 0))
+    mz = O.mz_loc(2)
+    parts = []
+    for i, (b1, ns) in enumerate(((0.5, 40), (2.0, 25), (4.0, 10))):
+        ev = SimEvent(*_pulse_train(23, -9.0 + i, 7.0 - i, n_pulses=2, n_samples=ns, b1=b1, rec=0.5))
+        parts.append(Experiment(p1, pad_events(ev, ev.dt.shape[1] + 3 * i), m0, mz))
+    zj = Experiment.stack(parts).simulate()
+    alone = [part.simulate() for part in parts]
+    for i, z in enumerate(alone):
+        np.testing.assert_array_equal(zj[i * 23:(i + 1) * 23], z)
+    # the same chains in the reverse stacking order: other warp neighbours again
+    zr = Experiment.stack(parts[::-1]).simulate()
+    for i, z in enumerate(alone[::-1]):
+        np.testing.assert_array_equal(zr[i * 23:(i + 1) * 23], z)
 
 
 def test_jacobian_matches_the_oracle_and_the_reference(cuda):

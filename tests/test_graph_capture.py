@@ -1,7 +1,8 @@
-"""The forward entry points inside a CUDA graph: after one call of the same size (which sizes the
-workspace and uploads the Taylor tables), bmc_simulate and bmc_uneven_simulate enqueue only kernels and
-asynchronous device work, so a caller can capture them and replay the graph; the replays reproduce the
-direct call bit for bit."""
+"""The forward entry points inside a CUDA graph: after one call of the same size on the capturing stream
+(which sizes that stream's workspace and uploads the Taylor tables), bmc_simulate and bmc_uneven_simulate
+enqueue only kernels and asynchronous device work, so a caller can capture them and replay the graph; the
+replays reproduce the direct call bit for bit. A capture whose stream has no workspace of the size yet is
+refused with a message (growing it would allocate inside the capture)."""
 import ctypes as C
 
 import numpy as np
@@ -40,6 +41,11 @@ def test_bmc_simulate_replays_from_a_graph(cuda):
     s = torch.cuda.Stream()
     s.wait_stream(torch.cuda.current_stream())
     with torch.cuda.stream(s):
+        with pytest.raises(RuntimeError, match="before capturing"):
+            with torch.cuda.graph(torch.cuda.CUDAGraph(), stream=s):
+                call()
+        call()                                   # sizes the workspace of the capturing stream
+        torch.cuda.synchronize()
         out.zero_()
         with torch.cuda.graph(g, stream=s):
             call()
