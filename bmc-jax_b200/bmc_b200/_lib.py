@@ -18,7 +18,7 @@ LIB_PATH = Path(__file__).resolve().parent / LIB_NAME
 
 MAX_CEST = 5
 MAX_TANGENTS = 8
-F64, F32 = 0, 1
+F64, F32, MIXED = 0, 1, 2
 SEED_NONE, SEED_SPREAD_SIGMA = -1, -2
 SLOT_SPREAD_SIGMA, SLOT_M_START = -2, -3
 

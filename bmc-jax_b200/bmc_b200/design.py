@@ -65,6 +65,9 @@ def fisher_information(experiment, spec: FitSpec, x, sigma):
 
 @dataclass(frozen=True)
 class CRLB:
+    """The bound at the values x (the fields of BMC-JAX design/crlb.py:61-85): per parameter the smallest
+    standard deviation an unbiased estimate can have (sd), the correlations, the Fisher matrix and the
+    Jacobian it came from."""
     names: tuple
     x: np.ndarray
     sd: np.ndarray
@@ -74,16 +77,20 @@ class CRLB:
 
     @property
     def rel_sd(self) -> np.ndarray:
-        return self.sd / np.abs(self.x)
+        """sd / |x|."""
+        return np.asarray(self.sd) / np.abs(np.asarray(self.x))
 
     def __getitem__(self, name: str) -> float:
-        return float(self.sd[self.names.index(name)])
+        """The bound (sd) of one parameter by its name (ValueError for a name not in the bound)."""
+        bound = dict(zip(self.names, np.asarray(self.sd)))
+        if name not in bound:
+            raise ValueError(f"{name!r} is not one of {self.names}")
+        return float(bound[name])
 
     def summary(self) -> str:
-        rows = [f"{'parameter':>10} {'value':>12} {'CRLB (SD)':>12} {'relative':>9}"]
-        for n, x, s, r in zip(self.names, self.x, self.sd, self.rel_sd):
-            rows.append(f"{n:>10} {x:>12.6g} {s:>12.4g} {100 * r:>8.2f}%")
-        return "\n".join(rows)
+        """One line per parameter: value, bound and the bound relative to the value."""
+        return "\n".join(f"{n}: {x:.6g} +- {s:.4g} (CRLB, {100 * r:.2f}% of the value)"
+                         for n, x, s, r in zip(self.names, self.x, self.sd, self.rel_sd))
 
 
 def crlb(experiment, spec: FitSpec, sigma, x=None) -> CRLB:

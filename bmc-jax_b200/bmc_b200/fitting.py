@@ -187,8 +187,28 @@ class Experiment:
 # ------------------------------------------------------------------------------------------------
 # what comes back (fitting/result.py)
 # ------------------------------------------------------------------------------------------------
+def _near(x, ref, rel, floor):
+    """|x - ref| <= floor + rel |ref|, elementwise (NaN compares False)."""
+    x, ref = np.asarray(x, np.float64), np.asarray(ref, np.float64)
+    return np.abs(x - ref) <= floor + rel * np.abs(ref)
+
+
+def _rms_rows(r):
+    """Root mean square over the last axis."""
+    r = np.asarray(r, np.float64)
+    return np.linalg.norm(r, axis=-1) / np.sqrt(max(r.shape[-1], 1))
+
+
 @dataclass(frozen=True)
 class FitResult:
+    """The outcome of `fit` / `fit_joint` (the fields of BMC-JAX fitting/result.py:23-174).
+
+    x (n_samples, n_params) fitted values in physical units; z_fit the model at x and z_meas the data it
+    was fitted to; spec the FitSpec (names, bounds). n_per_block: offsets per stacked experiment (for
+    rms_per_block). fit_joint also fills free (where a slot was fitted; elsewhere x holds the value the
+    sample carries), sd and corr (misfit-scaled standard deviations and correlations, NaN where not
+    free), x0, cost (after every step), nan_steps and blocks (per-experiment values, name -> dict of x,
+    sd and at_bounds; their column of x is NaN)."""
     x: np.ndarray
     z_fit: np.ndarray
     z_meas: np.ndarray
@@ -204,68 +224,80 @@ class FitResult:
 
     @property
     def names(self) -> List[str]:
-        return [s.name for s in self.spec.slots]
+        return [slot.name for slot in self.spec.slots]
 
     def __getitem__(self, name: str) -> np.ndarray:
-        if self.blocks and name in self.blocks:
+        """One parameter over the samples (a per-block parameter: over the experiments)."""
+        if name in (self.blocks or {}):
             return self.blocks[name]["x"]
-        try:
-            return self.x[:, self.names.index(name)]
-        except ValueError:
-            raise KeyError(f"no parameter {name!r}; the fit has {self.names}") from None
+        col = {nm: j for j, nm in enumerate(self.names)}.get(name)
+        if col is None:
+            raise KeyError(f"no parameter {name!r}; the fit has {self.names}")
+        return self.x[:, col]
 
     @property
     def residual(self) -> np.ndarray:
-        return self.z_fit - self.z_meas
+        """z_fit - z_meas."""
+        return np.asarray(self.z_fit) - np.asarray(self.z_meas)
 
     @property
     def rms(self) -> np.ndarray:
-        return np.sqrt(np.mean(self.residual ** 2, axis=-1))
+        return _rms_rows(self.residual)
 
     @property
     def rms_per_block(self):
+        """(n_samples, n_blocks) rms of every stacked experiment, or None without n_per_block."""
         if self.n_per_block is None:
             return None
-        nb = self.z_meas.shape[-1] // self.n_per_block
-        r = self.residual[..., :nb * self.n_per_block]
-        return np.sqrt(np.mean(r.reshape(*r.shape[:-1], nb, self.n_per_block) ** 2, axis=-1))
+        m = int(self.n_per_block)
+        r = self.residual
+        nb = r.shape[-1] // m
+        return np.stack([_rms_rows(r[..., b * m:(b + 1) * m]) for b in range(nb)], axis=-1)
+
+    def _only_free(self, mask):
+        return mask if self.free is None else mask & np.asarray(self.free, bool)
 
     @property
     def at_bounds(self) -> np.ndarray:
-        lo, hi = np.asarray(self.spec.lo_phys), np.asarray(self.spec.hi_phys)
-        railed = np.isclose(self.x, lo) | np.isclose(self.x, hi)
-        return railed if self.free is None else railed & self.free
+        """Fitted values that sit on a bound (within 1e-8 + 1e-5 of it): not measurements."""
+        lo = np.asarray(self.spec.lo_phys)[None, :]
+        hi = np.asarray(self.spec.hi_phys)[None, :]
+        return self._only_free(_near(self.x, lo, 1e-5, 1e-8) | _near(self.x, hi, 1e-5, 1e-8))
 
     @property
     def unmoved(self):
+        """Free values that never left their start (within 1e-6 relative), or None without x0."""
         if self.x0 is None:
             return None
-        still = np.isclose(self.x, self.x0, rtol=1e-6, atol=0.0)
-        return still if self.free is None else still & self.free
+        return self._only_free(_near(self.x, self.x0, 1e-6, 0.0))
 
     def summary(self) -> str:
-        head = f"{'sample':>6}  " + "  ".join(f"{n:>12}" for n in self.names) + f"  {'rms':>9}"
-        rows = [head, "-" * len(head)]
-        ab = self.at_bounds
-        for i in range(self.x.shape[0]):
+        """A text table: one line per sample, a flag after every value that is railed ([b]) or held
+        ([h]), then the per-experiment values."""
+        names = self.names
+        w = max([10] + [len(n) + 4 for n in names])
+        railed, held = self.at_bounds, (None if self.free is None else ~np.asarray(self.free, bool))
+        lines = [f"FitResult: {self.x.shape[0]} samples, mean rms {float(np.mean(self.rms)):.3e}",
+                 "sample | " + " ".join(n.rjust(w) for n in names) + " |       rms"]
+        for i, row in enumerate(np.asarray(self.x)):
             cells = []
-            for j, _ in enumerate(self.names):
-                mark = "*" if ab[i, j] else ("=" if self.free is not None and not self.free[i, j] else " ")
-                cells.append(f"{self.x[i, j]:>11.5g}{mark}")
-            rows.append(f"{i:>6}  " + "  ".join(cells) + f"  {self.rms[i]:>9.2e}")
-        if ab.any():
-            rows.append("* on a bound -- not a measurement, the optimiser was stopped there")
-        if self.free is not None and not self.free.all():
-            rows.append("= not free in this sample: the value its params carry")
-        for name, b in (self.blocks or {}).items():
-            rows.append(f"{name} per experiment: " + "  ".join(
-                f"{v:.5g}{'*' if r else ''}" for v, r in zip(b["x"], b["at_bounds"])))
-        return "\n".join(rows)
+            for j, v in enumerate(row):
+                tag = "[b]" if railed[i, j] else ("[h]" if held is not None and held[i, j] else "   ")
+                cells.append(f"{v:.5g}{tag}".rjust(w))
+            lines.append(f"{i:6d} | " + " ".join(cells) + f" | {self.rms[i]:9.2e}")
+        if railed.any() or (held is not None and held.any()):
+            lines.append("[b] on a bound: the optimiser was stopped there, not a measurement; "
+                         "[h] held: not free in this sample")
+        for name, blk in (self.blocks or {}).items():
+            vals = ", ".join(f"{v:.5g}" + (" [b]" if r else "") for v, r in zip(blk["x"], blk["at_bounds"]))
+            lines.append(f"{name} per experiment: {vals}")
+        return "\n".join(lines)
 
     def __repr__(self) -> str:
-        railed = int(self.at_bounds.sum())
-        return (f"FitResult({self.x.shape[0]} samples, {self.names}, "
-                f"rms {self.rms.mean():.3e}" + (f", {railed} at bounds)" if railed else ")"))
+        n_rail = int(np.count_nonzero(self.at_bounds))
+        tail = f", {n_rail} values on a bound" if n_rail else ""
+        return (f"<FitResult of {self.x.shape[0]} samples: {', '.join(self.names)}; "
+                f"mean rms {float(np.mean(self.rms)):.3e}{tail}>")
 
 
 # ------------------------------------------------------------------------------------------------
@@ -432,45 +464,114 @@ def fit(experiment: Experiment, spec: FitSpec, z_meas, n_iter=30, x0_phys=None, 
 # ------------------------------------------------------------------------------------------------
 # joint fits (fitting/joint.py)
 # ------------------------------------------------------------------------------------------------
-def _layout(spec: FitSpec, n: int, n_blocks: int):
-    """free (n, L); pos (L,); n_loc; cols [(slot, samples, block or -1)] per joint column."""
-    width = [n_blocks if s.scope == "block" else 1 for s in spec.slots]
-    pos = np.concatenate([[0], np.cumsum(width)[:-1]]).astype(int)
+@dataclass
+class _Columns:
+    """Where every free number of a joint fit lives.
+
+    Sample i's local vector has one entry per slot, or one per experiment for a per-block slot, the slot's
+    entries starting at pos[slot]. A joint column is one free number: a sample value (one sample), a
+    shared value (every sample it is free in) or one experiment's value of a per-block slot; `cols` lists
+    (slot, samples, experiment or -1) per column and col_of[i, j] names the column behind sample i's local
+    entry j (-1: held)."""
+    free: np.ndarray
+    pos: np.ndarray
+    n_loc: int
+    cols: list
+    col_of: np.ndarray
+
+
+def _columns(spec: FitSpec, n: int, n_blocks: int) -> _Columns:
+    widths = [n_blocks if sl.scope == "block" else 1 for sl in spec.slots]
+    pos = np.cumsum([0] + widths[:-1]).astype(int)
+    n_loc = int(sum(widths))
     free = np.zeros((n, spec.n), bool)
+    col_of = np.full((n, n_loc), -1, int)
     cols = []
-    for l, s in enumerate(spec.slots):
-        who = list(range(n)) if s.samples is None else list(s.samples)
-        missing = [i for i in who if not 0 <= i < n]
-        if missing:
-            raise ValueError(f"{s.name}: samples {missing} do not exist (the fit has {n})")
+    for l, sl in enumerate(spec.slots):
+        who = np.arange(n) if sl.samples is None else np.asarray(sl.samples, int)
+        outside = who[(who < 0) | (who >= n)]
+        if outside.size:
+            raise ValueError(f"{sl.name}: samples {outside.tolist()} do not exist (the fit has {n})")
         free[who, l] = True
-        if s.scope == "shared":
-            cols.append((l, who, -1))
-        elif s.scope == "block":
-            cols += [(l, who, b) for b in range(n_blocks)]
-        else:
-            cols += [(l, [i], -1) for i in who]
-    return free, pos, int(sum(width)), cols
+        if sl.scope == "sample":                 # one column per sample
+            for i in who.tolist():
+                col_of[i, pos[l]] = len(cols)
+                cols.append((l, [i], -1))
+        else:                                    # one column for all its samples, per experiment if "block"
+            for b in (range(n_blocks) if sl.scope == "block" else (-1,)):
+                col_of[who, pos[l] + max(b, 0)] = len(cols)
+                cols.append((l, who.tolist(), b))
+    return _Columns(free, pos, n_loc, cols, col_of)
 
 
 def _carried(params: SimParams, m0, spec: FitSpec, sig_held):
-    """(n, L): each slot's number where it is not free (joint.py:99-117)."""
+    """(n, L): the number each slot stands for where it is not free -- the field's own value, 1 for a
+    factor, 0 for an offset, the start state's water Mz over water_f for m_start, the held width for
+    b0_spread (fitting/joint.py:99-117)."""
     n = m0.shape[0]
-    nc = n_cest_of(params)
-    out = []
-    for s in spec.slots:
-        if s.field == "b0_spread":
-            out.append(np.asarray(sig_held, np.float64))
-        elif s.mode == "factor":
-            out.append(np.ones(n))
-        elif s.mode == "add":
-            out.append(np.zeros(n))
-        elif s.field == "m_start":
-            out.append(m0[:, 2 * (1 + nc)] / np.asarray(params.water_f, np.float64))
-        else:
-            a = np.asarray(getattr(params, s.field), np.float64)
-            out.append(a if s.index is None else a[:, s.index])
-    return np.stack(out, axis=1)
+    water_z = 2 * (1 + n_cest_of(params))
+    neutral = {"factor": 1.0, "add": 0.0}
+
+    def held(sl):
+        if sl.field == "b0_spread":
+            return np.broadcast_to(np.asarray(sig_held, np.float64), (n,))
+        if sl.mode in neutral:
+            return np.full(n, neutral[sl.mode])
+        if sl.field == "m_start":
+            return m0[:, water_z] / np.asarray(params.water_f, np.float64)
+        v = np.asarray(getattr(params, sl.field), np.float64)
+        return v if sl.index is None else v[:, sl.index]
+    return np.column_stack([held(sl) for sl in spec.slots])
+
+
+def _error_bars(Hl, resid, lay: _Columns, spec: FitSpec, coupled: bool, x_cols=None):
+    """Misfit-scaled standard deviations and correlations at the solution (fitting/joint.py:418-453), from
+    each sample's local normal matrix Hl[i] = J_i^T J_i: (sd (n, L), corr (n, L, L), per-block dict).
+
+    Independent samples: cov_i = pinv(H_i over its free slots) s_i^2 with s_i^2 = r_i.r_i / (points - free).
+    Coupled: J^T J over the joint columns is the sum of the samples' blocks placed at their columns, and
+    cov = pinv(J^T J) s^2 with s^2 = r.r / (all points - columns); a sample's slots read their columns."""
+    n, L = lay.free.shape
+    sd = np.full((n, L), np.nan)
+    corr = np.full((n, L, L), np.nan)
+
+    def bars(cov, scale):
+        var = np.clip(np.diag(cov), 0.0, None)
+        dev = np.sqrt(var)
+        with np.errstate(invalid="ignore", divide="ignore"):
+            return dev * scale, cov / (dev[:, None] * dev[None, :])
+    blocks = {}
+    if not coupled:
+        for i in range(n):
+            sl = np.flatnonzero(lay.free[i])
+            if not sl.size:
+                continue
+            H = Hl[i][np.ix_(lay.pos[sl], lay.pos[sl])]
+            s2 = float(resid[i] @ resid[i]) / max(resid.shape[1] - sl.size, 1)
+            sd[i, sl], corr[i][np.ix_(sl, sl)] = bars(np.linalg.pinv(H) * s2, spec.scales[sl])
+        return sd, corr, blocks
+    P = len(lay.cols)
+    JtJ = np.zeros((P, P))
+    for i in range(n):
+        ent = np.flatnonzero(lay.col_of[i] >= 0)
+        c = lay.col_of[i, ent]
+        np.add.at(JtJ, (c[:, None], c[None, :]), Hl[i][np.ix_(ent, ent)])
+    s2 = float(np.sum(resid * resid)) / max(resid.size - P, 1)
+    slot_of = np.array([l for l, _, _ in lay.cols], int)
+    sd_c, corr_c = bars(np.linalg.pinv(JtJ) * s2, spec.scales[slot_of])
+    is_block = np.array([sl.scope == "block" for sl in spec.slots])
+    for i in range(n):
+        sl = np.flatnonzero(lay.free[i] & ~is_block)
+        c = lay.col_of[i, lay.pos[sl]]
+        sd[i, sl] = sd_c[c]
+        corr[i][np.ix_(sl, sl)] = corr_c[np.ix_(c, c)]
+    for l in np.flatnonzero(is_block):
+        c = np.flatnonzero(slot_of == l)
+        vals = np.asarray(x_cols, np.float64)[c] * spec.scales[l]
+        sl = spec.slots[l]
+        blocks[sl.name] = dict(x=vals, sd=sd_c[c],
+                               at_bounds=_near(vals, sl.lo, 1e-5, 1e-8) | _near(vals, sl.hi, 1e-5, 1e-8))
+    return sd, corr, blocks
 
 
 class _JointModel:
@@ -727,13 +828,6 @@ def _joint_solve(Hl, gl, col_of, shared, P, lam, keep=None):
     return sol
 
 
-def _cov_to_sd_corr(cov, scale):
-    sd = np.sqrt(np.clip(np.diag(cov), 0.0, None))
-    with np.errstate(invalid="ignore", divide="ignore"):
-        corr = cov / np.outer(sd, sd)
-    return sd * scale, corr
-
-
 def fit_joint(experiment: Experiment, spec: FitSpec, z_meas, n_iter=30, x0_phys=None, n_per_block=None,
               max_chunk=None, lam0=1e-2, callback=None, spread=None, block_jacobian="full", stop_lam=None,
               active_bounds=False, keep_jacobian=False, _internals=False):
@@ -765,7 +859,8 @@ def fit_joint(experiment: Experiment, spec: FitSpec, z_meas, n_iter=30, x0_phys=
     if blocked and (not n_per_block or n_pts % n_per_block):
         raise ValueError(f"a per-block value needs n_per_block dividing the {n_pts} offsets (got {n_per_block})")
     nb = n_pts // n_per_block if blocked else 1
-    free, pos, n_loc, cols = _layout(spec, n, nb)
+    lay = _columns(spec, n, nb)
+    free, pos, n_loc, cols, col_of = lay.free, lay.pos, lay.n_loc, lay.cols, lay.col_of
     P = len(cols)
     L = spec.n
     scales = spec.scales
@@ -779,27 +874,24 @@ def fit_joint(experiment: Experiment, spec: FitSpec, z_meas, n_iter=30, x0_phys=
     model = _JointModel(params, m0, events, mz, spec, free, pos, n_loc, nb, n_per_block, spread,
                         sig_held if sig_held is not None else np.zeros(n))
     model.carried_in = carried
-    # joint column -> local entry of every sample
-    col_of = -np.ones((n, n_loc), int)
-    for p, (l, who, b) in enumerate(cols):
-        for i in who:
-            col_of[i, pos[l] + max(b, 0)] = p
+    i_ent, j_ent = np.nonzero(col_of >= 0)
+    c_ent = col_of[i_ent, j_ent]
 
     def locs(x):
+        """Every sample's local vector for the joint vector x (0 where the entry is held)."""
         loc = np.zeros((n, n_loc))
-        for p, (l, who, b) in enumerate(cols):
-            loc[who, pos[l] + max(b, 0)] = x[p]
+        loc[i_ent, j_ent] = np.asarray(x)[c_ent]
         return loc
 
     def resid(x):
         return (model.evaluate(locs(x), need_jac=False)[0] - z).reshape(-1)
 
     def jac(x):
+        """The dense joint Jacobian (points, columns): each sample's local columns placed at their joint
+        columns (a sample's entries map to distinct columns)."""
         Zm, Jl = model.evaluate(locs(x))
         J = np.zeros((n, n_pts, P))
-        for p, (l, who, b) in enumerate(cols):
-            for i in who:
-                J[i, :, p] += Jl[i, :, pos[l] + max(b, 0)]
+        J[i_ent, :, c_ent] = Jl[i_ent, :, j_ent]
         return J.reshape(-1, P)
 
     x_start = np.asarray([X0[who[0], l] / scales[l] for l, who, _ in cols], np.float64)
@@ -850,10 +942,7 @@ def fit_joint(experiment: Experiment, spec: FitSpec, z_meas, n_iter=30, x0_phys=
                 gl = np.einsum("inj,in->ij", Jl, r)
                 keep = None
                 if active_bounds:
-                    g_full = np.zeros(P)
-                    for i in range(n):
-                        u = np.flatnonzero(col_of[i] >= 0)
-                        np.add.at(g_full, col_of[i][u], gl[i][u])
+                    g_full = np.bincount(c_ent, weights=gl[i_ent, j_ent], minlength=P)
                     keep = np.where(((x <= lo) & (g_full > 0)) | ((x >= hi) & (g_full < 0)), 0.0, 1.0)
                 d = _joint_solve(Hl, gl, col_of, shared_cols, P, lam, keep)
                 xn = np.clip(x + d, lo, hi)
@@ -878,34 +967,8 @@ def fit_joint(experiment: Experiment, spec: FitSpec, z_meas, n_iter=30, x0_phys=
     X = np.where(free, loc[:, pos] * scales, carried)
     Zf, Jl = model.evaluate(loc)
     r_all = Zf - z
-    sd = np.full(free.shape, np.nan)
-    corr = np.full(free.shape + (L,), np.nan)
-    blocks = {}
-    if not coupled:
-        for i in range(n):
-            use = np.flatnonzero(free[i])
-            if use.size:
-                Ju = Jl[i][:, pos[use]]
-                s2 = float(r_all[i] @ r_all[i]) / max(r_all.shape[1] - use.size, 1)
-                sd[i, use], corr[i][np.ix_(use, use)] = _cov_to_sd_corr(np.linalg.pinv(Ju.T @ Ju) * s2, scales[use])
-    else:
-        J = np.zeros((n, n_pts, P))
-        for p, (l, who, b) in enumerate(cols):
-            for i in who:
-                J[i, :, p] += Jl[i, :, pos[l] + max(b, 0)]
-        J = J.reshape(-1, P)
-        s2 = float(np.sum(r_all ** 2)) / max(r_all.size - P, 1)
-        sd_col, corr_col = _cov_to_sd_corr(np.linalg.pinv(J.T @ J) * s2, col_scale)
-        for i in range(n):
-            ps = [p for p, (l, who, b) in enumerate(cols) if i in who and b < 0]
-            ls = col_slot[ps]
-            sd[i, ls] = sd_col[ps]
-            corr[i][np.ix_(ls, ls)] = corr_col[np.ix_(ps, ps)]
-        for l in np.flatnonzero(is_block):
-            ps = [p for p, (ll, _, b) in enumerate(cols) if ll == l]
-            xb = np.asarray(x, float)[ps] * scales[l]
-            blocks[spec.slots[l].name] = dict(x=xb, sd=sd_col[ps], at_bounds=(
-                np.isclose(xb, spec.slots[l].lo) | np.isclose(xb, spec.slots[l].hi)))
+    sd, corr, blocks = _error_bars(np.einsum("inj,ink->ijk", Jl, Jl), r_all, lay, spec, coupled,
+                                   x if coupled else None)
     X[:, is_block] = np.nan
     X0 = np.where(is_block[None, :], np.nan, X0)
     free = free & ~is_block[None, :]

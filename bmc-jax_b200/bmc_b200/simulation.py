@@ -231,7 +231,8 @@ def _device(a, dtype=np.float64):
 
 
 def problem(n_vox, n_off, n_ev, n_cest, mz, precision=None, reset_after_adc=True):
-    prec = (_lib.F64 if settings.x64_enabled() else _lib.F32) if precision is None else precision
+    prec = {"f64": _lib.F64, "mixed": _lib.MIXED, "f32": _lib.F32}[settings.precision()] if precision is None \
+        else precision
     return _lib.Problem(n_vox, n_off, n_ev, n_cest, mz, 1 if reset_after_adc else 0, prec, 0)
 
 

@@ -277,12 +277,18 @@ class LadderWarmStart:
         return np.clip(x, np.maximum(self.spec.lo_phys, self.lo), np.minimum(self.spec.hi_phys, self.hi))
 
     def fit(self, z_meas, n_iter_warm: int = 8, n_iter_plain: int = 30,
-            fallback_rms: Optional[float] = None) -> WarmFitResult:
-        """LM from the network's starting values (n_iter_warm iterations); voxels whose rms ends above
-        `fallback_rms` (default 1.5 sigma, at least 1e-4) are refitted from the FitSpec's x0 with
-        n_iter_plain iterations and keep the better of the two fits."""
+            fallback_rms: Optional[float] = None, judge: str = "threshold") -> WarmFitResult:
+        """LM from the network's starting values (n_iter_warm iterations), with the plain fit from the
+        FitSpec's x0 (n_iter_plain iterations) as the fallback; a voxel refitted plainly keeps the better
+        (lower rms) of its two fits.
+
+        judge="threshold": only voxels whose warm rms ends above `fallback_rms` (default 1.5 sigma, at
+        least 1e-4) are refitted -- the fast rule. judge="plain": every voxel is also fitted plainly, so
+        no voxel keeps a warm fit whose rms is above its plain fit's (costs the whole plain fit)."""
         import time
         from .fitting import fit
+        if judge not in ("threshold", "plain"):
+            raise ValueError(f"judge {judge!r}; use 'threshold' or 'plain'")
         z = np.atleast_2d(np.asarray(z_meas, np.float64))
         thr = fallback_rms if fallback_rms is not None else max(1.5 * self.sigma, 1e-4)
         t0 = time.perf_counter()
@@ -291,7 +297,7 @@ class LadderWarmStart:
         warm = fit(self.experiment, self.spec, z, n_iter=n_iter_warm, x0_phys=x0)
         t2 = time.perf_counter()
         x, rms = warm.x.copy(), warm.rms.copy()
-        bad = np.flatnonzero(~(rms <= thr))
+        bad = np.flatnonzero(~(rms <= thr)) if judge == "threshold" else np.arange(z.shape[0])
         if bad.size:
             plain = fit(self.experiment, self.spec, z[bad], n_iter=n_iter_plain)
             better = ~(warm.rms[bad] <= plain.rms)

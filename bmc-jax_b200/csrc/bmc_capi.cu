@@ -100,7 +100,23 @@ TaylorTable make_table(double tol, int m_max, double dense_theta, double dense_s
     return t;
 }
 
-__device__ TaylorTable g_tables[2];   // [BMC_F64, BMC_F32], per device
+// The mixed precision's Taylor tolerance and float32 threshold (BMC_MIXED in include/bmc_b200.h); a
+// build may set others with -D for a sweep.
+#ifndef BMC_MIXED_TOL
+#define BMC_MIXED_TOL 1e-10
+#endif
+#ifndef BMC_MIXED_F32
+#define BMC_MIXED_F32 0.3
+#endif
+
+__device__ TaylorTable g_tables[3];   // [BMC_F64, BMC_F32, BMC_MIXED], per device
+
+// the three tables, in precision order
+void host_tables(TaylorTable* h) {
+    h[BMC_F64] = make_table(1e-13, 30, 0.5, 100.0, 1e-6);
+    h[BMC_F32] = make_table(std::ldexp(1.0, -24), 16, 0.5, 100.0, 0.0);
+    h[BMC_MIXED] = make_table(BMC_MIXED_TOL, 30, 0.5, 100.0, BMC_MIXED_F32);
+}
 
 struct DeviceState {
     bool tables_ready = false;
@@ -128,13 +144,13 @@ bmc_status tables(int precision, const TaylorTable** out) {
     std::lock_guard<std::mutex> lk(g_mu);
     DeviceState& ds = dev_state(dev);
     if (!ds.tables_ready) {
-        TaylorTable h[2] = {make_table(1e-13, 30, 0.5, 100.0, 1e-6),
-                            make_table(std::ldexp(1.0, -24), 16, 0.5, 100.0, 0.0)};
+        TaylorTable h[3];
+        host_tables(h);
         CUDA_TRY(cudaMemcpyToSymbol(g_tables, h, sizeof(h)));
         CUDA_TRY(cudaGetSymbolAddress((void**)&ds.tables, g_tables));
         ds.tables_ready = true;
     }
-    *out = ds.tables + (precision == BMC_F32 ? 1 : 0);
+    *out = ds.tables + precision;
     return BMC_OK;
 }
 
@@ -190,8 +206,8 @@ bmc_status check_problem(const bmc_problem* pr, const double* params, const bmc_
         return fail(BMC_ERR_UNSUPPORTED, "n_cest %d outside 0..%d", pr->n_cest, BMC_MAX_CEST);
     const int N = 3 * (1 + pr->n_cest) + 1;
     if (pr->mz_loc >= N) return fail(BMC_ERR_INVALID, "mz_loc %d outside the state (size %d)", pr->mz_loc, N);
-    if (pr->precision != BMC_F64 && pr->precision != BMC_F32)
-        return fail(BMC_ERR_INVALID, "precision %d is neither BMC_F64 nor BMC_F32", pr->precision);
+    if (pr->precision != BMC_F64 && pr->precision != BMC_F32 && pr->precision != BMC_MIXED)
+        return fail(BMC_ERR_INVALID, "precision %d is not BMC_F64, BMC_F32 or BMC_MIXED", pr->precision);
     if (pr->n_events > 0 && (!ev->d_type || !ev->d_dt || !ev->d_rf_amp || !ev->d_rf_phase || !ev->d_rf_freq))
         return fail(BMC_ERR_INVALID, "null event field");
     return BMC_OK;
@@ -938,7 +954,8 @@ bmc_status noalloc_setup(int precision, void** scratch, const TaylorTable** tt) 
         return fail(BMC_ERR_UNSUPPORTED, "bmc_simulate_noalloc: device %d above %d", dev, kNoAllocMaxDevices - 1);
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
     if (!g_noalloc_tables[dev]) {
-        TaylorTable h[2] = {make_table(1e-13, 30, 0.5, 100.0, 1e-6), make_table(std::ldexp(1.0, -24), 16, 0.5, 100.0, 0.0)};
+        TaylorTable h[3];
+        host_tables(h);
         CUDA_TRY(cudaMemcpyToSymbol(g_tables, h, sizeof(h)));
         g_noalloc_tables[dev] = true;
     }
@@ -952,7 +969,7 @@ bmc_status noalloc_setup(int precision, void** scratch, const TaylorTable** tt) 
     }
     TaylorTable* t = nullptr;
     CUDA_TRY(cudaGetSymbolAddress((void**)&t, g_tables));
-    *tt = t + (precision == BMC_F32 ? 1 : 0);
+    *tt = t + precision;
     *scratch = g_noalloc_ptr[dev];
     return BMC_OK;
 }

@@ -27,8 +27,9 @@ struct TaylorTable {
     double dense_theta;    // dense path: ||X / 2^s|| <= dense_theta ...
     int dense_m;           // ... with this Horner degree
     double dense_switch;   // warps whose largest ||X|| exceeds this take the dense path
-    // float64 kernels: for a warp of Taylor degree m, the terms from f32_from[m] on are below 1e-6 of
-    // the state (theta[m]^k / k! <= 1e-6) and are formed in float32 (> m: none)
+    // float64 kernels: for a chain of Taylor degree m, the terms from f32_from[m] on are below the
+    // table's float32 threshold of the state (theta[m]^k / k! <= 1e-6 for BMC_F64, 0.3 for BMC_MIXED)
+    // and are formed in float32 (> m: none)
     int f32_from[kTaylorMMax + 1];
     float inv_fact_f[kTaylorMMax + 1];  // 1 / k! in float32
 };
@@ -54,8 +55,9 @@ struct ChainArgs {
     double* jout;              // [P][n_vox][n_off] or null
     double* traj;              // [n_vox][n_off][n_ev][N] or null: the state after every event
     int* status;               // error flags (bit 0: non-finite norm)
-    unsigned long long* work;  // null, or [4]: useful Taylor terms, dense Horner column products,
-                               // dense squarings, Taylor terms executed (warp maximum)
+    unsigned long long* work;  // null, or [5]: useful Taylor terms, dense Horner column products,
+                               // dense squarings, Taylor terms executed (warp maximum), and of the
+                               // useful Taylor terms those formed in float32
     // uneven batches (chain_kernel<..., true>): every voxel has its own event table
     long long n_chains;        // chains of the launch (canonical order: voxel-major, then row)
     const int2* chain_map;     // [n_chains]: (voxel, row of its table)

@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
     if (__all_sync(kFull, !act)) return;
 
     const size_t ch = UNEVEN ? (size_t)ci : (size_t)v * a.n_off + o;
-    unsigned wk0 = 0, wk1 = 0, wk2 = 0, wk3 = 0;   // this chain's work counts (each < 2^32 per launch)
+    unsigned wk0 = 0, wk1 = 0, wk2 = 0, wk3 = 0, wk4 = 0;   // this chain's work counts (each < 2^32 per launch)
     const bool count = a.work != nullptr;
     ChainConst<NC, D>& cc = reinterpret_cast<ChainConst<NC, D>*>(smem_raw + 4 * sizeof(SM))[threadIdx.x];
     for (int node = 0; node < a.n_nodes; ++node) {
@@ -391,7 +391,12 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
                 if (ns_w > 0) {
                     const R h = tay ? (ns_own == 1 ? rec.dt : rec.dt / R(ns_own)) : R(0);
                     const int passes = C::taylor_apply(cc, rec, g, h, ns_w, m_w, ns_own, m_own, M, tt);
-                    if (count && tay) wk0 += unsigned(ns_own * m_own);
+                    if (count && tay) {
+                        wk0 += unsigned(ns_own * m_own);
+                        // of those, the terms formed in float32 (all of them in the float32 kernel)
+                        const int k32 = std::is_same<R, float>::value ? 1 : (NT == 0 ? tt.f32_from[m_own] : m_own + 1);
+                        wk4 += unsigned(ns_own * (m_own + 1 - k32));
+                    }
                     if (count) wk3 += unsigned(passes * m_w);
                 }
             }
@@ -431,8 +436,9 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
     }
     if (a.work) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            unsigned long long x = act ? (unsigned long long)(q == 0 ? wk0 : (q == 1 ? wk1 : (q == 2 ? wk2 : wk3))) : 0ull;
+        for (int q = 0; q < 5; ++q) {
+            const unsigned wq = q == 0 ? wk0 : (q == 1 ? wk1 : (q == 2 ? wk2 : (q == 3 ? wk3 : wk4)));
+            unsigned long long x = act ? (unsigned long long)wq : 0ull;
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(kFull, x, off);
             if (lane == 0 && x) atomicAdd(a.work + q, x);

@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define BMC_ABI_VERSION 1
+#define BMC_ABI_VERSION 2
 #define BMC_MAX_CEST 5             /* water + up to five CEST pools + MT: N <= 19 */
 #define BMC_MAX_TANGENTS 8
 #define BMC_N_FIELDS(n_cest) (13 + 5 * (n_cest))
@@ -54,9 +54,15 @@ typedef enum {
  * tangents the Taylor terms below 1e-6 of the state (by the series bound) are formed in float32 and
  * added to the float64 state once per sub-step, at most ~2e-13 of the state per event. Tangents, the
  * dense path for long events and the LM arithmetic are float64 throughout. BMC_F32: float32 Taylor
- * propagation, float64 dense path. */
+ * propagation, float64 dense path (about 1e-4 in Z over thousands of pulse samples, the level of the
+ * reference's own float32 path). BMC_MIXED: the state and the leading Taylor terms of every sub-step in
+ * float64, every term below 0.3 of the state (by the series bound) formed in float32, and a truncation
+ * tolerance of 1e-10 per sub-step: the float32 rounding enters only through terms a few tenths of the
+ * state and smaller, and the state itself is never rounded to float32. Forward model only; float64
+ * dense path. */
 #define BMC_F64 0
 #define BMC_F32 1
+#define BMC_MIXED 2
 
 /* special tangent seeds (bmc_tangents.field_row) */
 #define BMC_SEED_NONE (-1)         /* only d_dm0 drives this tangent */
@@ -69,7 +75,7 @@ typedef struct {
     int32_t n_cest;                /* 0 .. BMC_MAX_CEST */
     int32_t mz_loc;                /* state index returned as Z; < 0 returns the full state */
     int32_t reset_after_adc;       /* 1: the state returns to M0 after every ADC (reference default) */
-    int32_t precision;             /* BMC_F64 or BMC_F32 */
+    int32_t precision;             /* BMC_F64, BMC_F32 or BMC_MIXED */
     int32_t reserved;
 } bmc_problem;
 
@@ -305,11 +311,11 @@ bmc_status bmc_mlp_adam_step(const bmc_mlp_shape* shape, float* d_params, const 
 
 /*
  * Diagnostics (no counterpart in the reference: measurement support for the benchmark).
- * bmc_simulate_counted: bmc_simulate that also adds the work it executed to d_work[4] (device,
+ * bmc_simulate_counted: bmc_simulate that also adds the work it executed to d_work[5] (device,
  *   zeroed by the caller): [0] Taylor sub-step terms each chain needed (one sparse operator product
  *   each), [1] dense-path Horner column products, [2] dense-path squarings, [3] Taylor terms executed
- *   (a warp runs to the largest need among its chains).
- * bmc_simulate_jvp_counted: bmc_simulate_jvp that adds the same four counts to d_work[4], summed over
+ *   (a warp runs to the largest need among its chains), [4] of the terms in [0], those formed in float32.
+ * bmc_simulate_jvp_counted: bmc_simulate_jvp that adds the same five counts to d_work[5], summed over
  *   its launches: one per tangent (two per launch for at most one CEST pool), each carrying the primal
  *   and its tangents through the same steps as dual numbers.
  * bmc_probe_fma_peak: launches `blocks` x 256 threads of 8 independent FMA chains x `iters`

@@ -1,9 +1,8 @@
 """Generate the golden vectors in this folder by EXECUTING THE REFERENCE'S OWN SOURCE.
 
-Run in a container where the BMC-JAX source tree is available (default /root/reference/src, or
-pass its `src` folder as argv[1]):
+Run where the BMC-JAX source tree is available, passing its `src` folder:
 
-    python tests/golden/make_golden.py [/path/to/BMC-JAX/src]
+    python tests/golden/make_golden.py /path/to/BMC-JAX/src
 
 JAX is not installable here, so `_jaxshim/jax` stands in for the JAX API subset the reference uses,
 eagerly and in float64 (see its docstring). Everything below calls reference functions by their
@@ -24,7 +23,9 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REF_SRC = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
+if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_golden.py /path/to/BMC-JAX/src")
+REF_SRC = sys.argv[1]
 sys.path.insert(0, str(HERE / "_jaxshim"))
 sys.path.insert(0, REF_SRC)
 
