@@ -109,12 +109,12 @@ def lib():
         i32p = C.POINTER(C.c_int32)
         L.bmc_uneven_create.argtypes = [C.c_int32, C.c_int32, i32p, C.POINTER(TableSet), C.c_int32, C.c_int32,
                                         C.POINTER(C.c_void_p), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
-        L.bmc_uneven_simulate.argtypes = [vp, vp, vp, C.POINTER(Spread), C.POINTER(Tangents), vp, vp, vp]
+        L.bmc_uneven_simulate.argtypes = [vp, vp, vp, C.POINTER(Spread), C.POINTER(Tangents), vp, vp, vp, vp]
         L.bmc_uneven_destroy.argtypes = [vp]
         L.bmc_normal_segments.argtypes = [C.c_int32, C.c_int32, C.c_int64, vp, vp, vp, vp, vp, vp, vp]
-        L.bmc_schur_step.argtypes = [C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, C.c_double, vp, vp, vp, vp]
-        L.bmc_schur_eliminate.argtypes = [C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, C.c_double, vp, vp, vp]
-        L.bmc_schur_back.argtypes = [C.c_int32, C.c_int32, C.c_int32, vp, C.c_double, vp, vp, vp, vp]
+        L.bmc_schur_step.argtypes = [C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, C.c_double, vp, vp, vp, vp, vp]
+        L.bmc_schur_eliminate.argtypes = [C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, C.c_double, vp, vp, vp, vp]
+        L.bmc_schur_back.argtypes = [C.c_int32, C.c_int32, C.c_int32, vp, C.c_double, vp, vp, vp, vp, vp]
         for f in ("bmc_uneven_create", "bmc_uneven_simulate", "bmc_uneven_destroy", "bmc_normal_segments",
                   "bmc_schur_step", "bmc_schur_eliminate", "bmc_schur_back"):
             getattr(L, f).restype = C.c_int

@@ -230,6 +230,14 @@ bmc_status fill_spread(ChainArgs& a, const bmc_spread* sp) {
     return BMC_OK;
 }
 
+// the repeated block of every row of a table of records (block_scan_kernel), into seg[n_rows]
+bmc_status scan_blocks(const EvRec<double>* rec, int n_rows, int n_ev, int stride, int4* seg, cudaStream_t st) {
+    if (n_rows <= 0) return BMC_OK;
+    block_scan_kernel<double><<<(n_rows + 63) / 64, 64, 0, st>>>(rec, n_rows, n_ev, stride, seg);
+    CUDA_TRY(cudaGetLastError());
+    return BMC_OK;
+}
+
 template <typename R>
 bmc_status prep_events(const bmc_problem* pr, const bmc_events* ev, EvRec<R>* out, cudaStream_t st) {
     const size_t n = (size_t)pr->n_offsets * pr->n_events;
@@ -344,6 +352,8 @@ struct UnevenPlan {
     long long* tab_base = nullptr;
     int* tab_noff = nullptr;
     int* tab_nev = nullptr;
+    int4* seg = nullptr;       // the repeated block of every row of every table
+    int* tab_row0 = nullptr;   // first row of each table in seg
     void* scratch = nullptr;   // sort keys and indices, cub scratch, status word
     size_t scratch_bytes = 0;
 };
@@ -355,7 +365,7 @@ struct Impl {
     // one simulation (or tangent set) of an uneven batch: chains sorted by estimated cost, outputs
     // in canonical chain order (voxel-major, then table row)
     static bmc_status uneven(const UnevenPlan& pl, const double* params, const double* m0, const bmc_spread* sp,
-                             const bmc_tangents* tg, double* z, double* jz, cudaStream_t st) {
+                             const bmc_tangents* tg, const int32_t* active, double* z, double* jz, cudaStream_t st) {
         const TaylorTable* tt = nullptr;
         bmc_status s = tables(BMC_F64, &tt);
         if (s != BMC_OK) return s;
@@ -367,6 +377,7 @@ struct Impl {
         a.ev = pl.rec;
         a.n_chains = pl.n_chains; a.chain_map = pl.chain_map; a.vox_table = pl.vox_table;
         a.tab_base = pl.tab_base; a.tab_noff = pl.tab_noff; a.tab_nev = pl.tab_nev;
+        a.seg = pl.seg; a.tab_row0 = pl.tab_row0; a.active = active;
         Carve cv(pl.scratch);
         a.status = cv.take<int>(1);
         CUDA_TRY(cudaMemsetAsync(a.status, 0, sizeof(int), st));
@@ -401,7 +412,9 @@ struct Impl {
         void* ws = nullptr;
         const size_t recb = pr->precision == BMC_F32 ? sizeof(EvRec<float>) : sizeof(EvRec<double>);
         const long long nch = (long long)pr->n_voxels * pr->n_offsets;
-        if ((s = workspace(align256(nrec * recb) + 256 + order_bytes(nch), st, &ws)) != BMC_OK) return s;
+        if ((s = workspace(align256(nrec * recb) + 256 + align256(sizeof(int4) * pr->n_offsets) + order_bytes(nch), st,
+                           &ws)) != BMC_OK)
+            return s;
         Carve cv(ws);
         ChainArgs a{};
         a.n_vox = pr->n_voxels; a.n_off = pr->n_offsets; a.n_ev = pr->n_events; a.n_fields = Layout<NC>::NF;
@@ -420,6 +433,9 @@ struct Impl {
         EvRec<double>* rec = cv.take<EvRec<double>>(nrec);
         if ((s = prep_events<double>(pr, ev, rec, st)) != BMC_OK) return s;
         a.ev = rec;
+        a.seg = cv.take<int4>(pr->n_offsets);
+        if ((s = scan_blocks(rec, pr->n_offsets, pr->n_events, pr->n_offsets, const_cast<int4*>(a.seg), st)) != BMC_OK)
+            return s;
         if ((s = order_chains<NC, double>(a, cv, st)) != BMC_OK) return s;
         return launch_chain<NC, double, 0>(a, tt, st);
     }
@@ -456,7 +472,9 @@ struct Impl {
         const size_t nrec = (size_t)pr->n_offsets * pr->n_events;
         void* ws = nullptr;
         const long long nch = (long long)pr->n_voxels * pr->n_offsets;
-        if ((s = workspace(align256(nrec * sizeof(EvRec<double>)) + 256 + order_bytes(nch), st, &ws)) != BMC_OK) return s;
+        if ((s = workspace(align256(nrec * sizeof(EvRec<double>)) + 256 + align256(sizeof(int4) * pr->n_offsets) +
+                               order_bytes(nch), st, &ws)) != BMC_OK)
+            return s;
         Carve cv(ws);
         ChainArgs a{};
         a.n_vox = pr->n_voxels; a.n_off = pr->n_offsets; a.n_ev = pr->n_events; a.n_fields = Layout<NC>::NF;
@@ -470,6 +488,9 @@ struct Impl {
         EvRec<double>* rec = cv.take<EvRec<double>>(nrec);
         if ((s = prep_events<double>(pr, ev, rec, st)) != BMC_OK) return s;
         a.ev = rec;
+        a.seg = cv.take<int4>(pr->n_offsets);
+        if ((s = scan_blocks(rec, pr->n_offsets, pr->n_events, pr->n_offsets, const_cast<int4*>(a.seg), st)) != BMC_OK)
+            return s;
         if ((s = order_chains<NC, double>(a, cv, st)) != BMC_OK) return s;
         return run_tangents<NC>(a, tg->n_tangents, tt, st);
     }
@@ -488,7 +509,8 @@ struct Impl {
                              align256(sizeof(double) * P * nv) + align256(sizeof(double) * P * nv * N) +
                              2 * align256(sizeof(double) * nv * no) + align256(sizeof(double) * P * nv * no) +
                              2 * align256(sizeof(double) * nv * P) + 2 * align256(sizeof(double) * nv) +
-                             align256(sizeof(int) * nv) + 4096 + order_bytes((long long)nv * no);
+                             align256(sizeof(int) * nv) + align256(sizeof(int4) * no) + 4096 +
+                             order_bytes((long long)nv * no);
         void* ws = nullptr;
         if ((s = workspace(bytes, st, &ws)) != BMC_OK) return s;
         Carve cv(ws);
@@ -509,6 +531,7 @@ struct Impl {
         double* lam = cv.take<double>(nv);
         double* cost = cv.take<double>(nv);
         int* need = cv.take<int>(nv);
+        int4* seg = cv.take<int4>(no);
         int* status = cv.take<int>(1);
         if ((s = prep_events<double>(pr, ev, rec, st)) != BMC_OK) return s;
         CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), st));
@@ -531,7 +554,8 @@ struct Impl {
         a.mz = pr->mz_loc; a.reset_after_adc = pr->reset_after_adc;
         if ((s = fill_spread(a, sp)) != BMC_OK) return s;
         const double* sig0 = sp ? sp->d_sigma_hz : nullptr;
-        a.ev = rec; a.status = status;
+        a.ev = rec; a.status = status; a.seg = seg;
+        if ((s = scan_blocks(rec, no, pr->n_events, no, seg, st)) != BMC_OK) return s;
         a.params = params; a.m0 = m0;
         if ((s = order_chains<NC, double>(a, cv, st)) != BMC_OK) return s;
         for (int p = 0; p < P; ++p) a.field_row[p] = fs->field_row[p] == BMC_SLOT_M_START ? BMC_SEED_NONE : fs->field_row[p];
@@ -768,6 +792,12 @@ bmc_status bmc_uneven_create(int32_t n_cest, int32_t n_voxels, const int32_t* h_
     };
     cudaError_t e = cudaGetDevice(&pl->dev);
     std::vector<int> noff(tabs->h_n_offsets, tabs->h_n_offsets + nt), nev(tabs->h_n_events, tabs->h_n_events + nt);
+    std::vector<int> row0(nt);
+    long long n_rows = 0;
+    for (int t = 0; t < nt; ++t) {
+        row0[t] = (int)n_rows;
+        n_rows += noff[t];
+    }
     pl->scratch_bytes = 256 + order_bytes(nch);
     if (e == cudaSuccess) e = cudaMalloc(&pl->rec, sizeof(EvRec<double>) * std::max<long long>(nrec, 1));
     if (e == cudaSuccess) e = cudaMalloc(&pl->chain_map, sizeof(int2) * std::max<long long>(nch, 1));
@@ -776,6 +806,9 @@ bmc_status bmc_uneven_create(int32_t n_cest, int32_t n_voxels, const int32_t* h_
     if (e == cudaSuccess) e = cudaMalloc(&pl->tab_noff, sizeof(int) * nt);
     if (e == cudaSuccess) e = cudaMalloc(&pl->tab_nev, sizeof(int) * nt);
     if (e == cudaSuccess) e = cudaMalloc(&pl->scratch, pl->scratch_bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&pl->seg, sizeof(int4) * std::max<long long>(n_rows, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&pl->tab_row0, sizeof(int) * nt);
+    if (e == cudaSuccess) e = cudaMemcpy(pl->tab_row0, row0.data(), sizeof(int) * nt, cudaMemcpyHostToDevice);
     if (e == cudaSuccess && nch) e = cudaMemcpy(pl->chain_map, cm.data(), sizeof(int2) * nch, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(pl->vox_table, h_voxel_table, sizeof(int) * n_voxels, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(pl->tab_base, base.data(), sizeof(long long) * nt, cudaMemcpyHostToDevice);
@@ -792,6 +825,13 @@ bmc_status bmc_uneven_create(int32_t n_cest, int32_t n_voxels, const int32_t* h_
                                                     tabs->ev.d_rf_amp + b, tabs->ev.d_rf_phase + b,
                                                     tabs->ev.d_rf_freq + b, pl->rec + b);
     }
+    for (int t = 0; t < nt; ++t) {
+        if (e == cudaSuccess && nev[t] > 0)
+            block_scan_kernel<double><<<(noff[t] + 63) / 64, 64>>>(pl->rec + base[t], noff[t], nev[t], noff[t],
+                                                                   pl->seg + row0[t]);
+        else if (e == cudaSuccess)
+            e = cudaMemset(pl->seg + row0[t], 0, sizeof(int4) * noff[t]);
+    }
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return undo(fail(BMC_ERR_CUDA, "uneven plan: %s", cudaGetErrorString(e)));
@@ -802,8 +842,8 @@ bmc_status bmc_uneven_create(int32_t n_cest, int32_t n_voxels, const int32_t* h_
 }
 
 bmc_status bmc_uneven_simulate(const void* plan, const double* d_params, const double* d_m0,
-                               const bmc_spread* spread, const bmc_tangents* tangents, double* d_z, double* d_jz,
-                               void* stream) {
+                               const bmc_spread* spread, const bmc_tangents* tangents, const int32_t* d_active,
+                               double* d_z, double* d_jz, void* stream) {
     if (!plan || !d_params || !d_m0 || !d_z) return fail(BMC_ERR_INVALID, "uneven: null plan, params, m0 or z");
     const UnevenPlan* pl = static_cast<const UnevenPlan*>(plan);
     int dev = 0;
@@ -819,13 +859,14 @@ bmc_status bmc_uneven_simulate(const void* plan, const double* d_params, const d
                 return fail(BMC_ERR_INVALID, "tangent %d: field row %d outside %d..%d", t, tangents->field_row[t], lo,
                             nf - 1);
     }
-    BMC_DISPATCH(pl->n_cest, uneven(*pl, d_params, d_m0, spread, tangents, d_z, d_jz, (cudaStream_t)stream));
+    BMC_DISPATCH(pl->n_cest, uneven(*pl, d_params, d_m0, spread, tangents, d_active, d_z, d_jz, (cudaStream_t)stream));
 }
 
 bmc_status bmc_uneven_destroy(void* plan) {
     UnevenPlan* pl = static_cast<UnevenPlan*>(plan);
     if (!pl) return BMC_OK;
-    void* ptrs[] = {pl->rec, pl->chain_map, pl->vox_table, pl->tab_base, pl->tab_noff, pl->tab_nev, pl->scratch};
+    void* ptrs[] = {pl->rec, pl->chain_map, pl->vox_table, pl->tab_base, pl->tab_noff, pl->tab_nev, pl->scratch,
+                    pl->seg, pl->tab_row0};
     cudaError_t first = cudaSuccess;
     for (void* p : ptrs) {
         if (!p) continue;
@@ -852,33 +893,33 @@ bmc_status bmc_normal_segments(int32_t n_voxels, int32_t n_params, int64_t n_cha
 }
 
 bmc_status bmc_schur_step(int32_t n_voxels, int32_t n_local, int32_t n_shared, const double* d_H, const double* d_g,
-                          const double* d_free, double lam, double* d_dx_local, double* d_dx_shared, double* d_work,
-                          void* stream) {
+                          const double* d_free, double lam, const double* d_lam, double* d_dx_local,
+                          double* d_dx_shared, double* d_work, void* stream) {
     if (n_voxels < 1 || n_local < 1 || n_local > kMaxJointP - 1 || (n_shared != 0 && n_shared != 1))
         return fail(BMC_ERR_INVALID, "schur step: %d voxels, %d local (1..%d) and %d shared (0 or 1) values",
                     n_voxels, n_local, kMaxJointP - 1, n_shared);
     if (!d_H || !d_g || !d_dx_local || !d_dx_shared || !d_work) return fail(BMC_ERR_INVALID, "schur step: null pointer");
-    if (!(lam >= 0.0)) return fail(BMC_ERR_INVALID, "schur step: damping %g", lam);
+    if (!d_lam && !(lam >= 0.0)) return fail(BMC_ERR_INVALID, "schur step: damping %g", lam);
     double* sums = d_work + (size_t)n_voxels * (2 * n_local + 4);
-    bmc_status s = bmc_schur_eliminate(n_voxels, n_local, n_shared, d_H, d_g, d_free, lam, d_work, sums, stream);
+    bmc_status s = bmc_schur_eliminate(n_voxels, n_local, n_shared, d_H, d_g, d_free, lam, d_lam, d_work, sums, stream);
     if (s != BMC_OK) return s;
-    return bmc_schur_back(n_voxels, n_local, n_shared, sums, lam, d_work, d_dx_local, d_dx_shared, stream);
+    return bmc_schur_back(n_voxels, n_local, n_shared, sums, lam, d_lam, d_work, d_dx_local, d_dx_shared, stream);
 }
 
 bmc_status bmc_schur_eliminate(int32_t n_voxels, int32_t n_local, int32_t n_shared, const double* d_H,
-                               const double* d_g, const double* d_free, double lam, double* d_work, double* d_sums,
-                               void* stream) {
+                               const double* d_g, const double* d_free, double lam, const double* d_lam,
+                               double* d_work, double* d_sums, void* stream) {
     if (n_voxels < 1 || n_local < 1 || n_local > kMaxJointP - 1 || (n_shared != 0 && n_shared != 1))
         return fail(BMC_ERR_INVALID, "schur step: %d voxels, %d local (1..%d) and %d shared (0 or 1) values",
                     n_voxels, n_local, kMaxJointP - 1, n_shared);
     if (!d_H || !d_g || !d_work || !d_sums) return fail(BMC_ERR_INVALID, "schur step: null pointer");
-    if (!(lam >= 0.0)) return fail(BMC_ERR_INVALID, "schur step: damping %g", lam);
+    if (!d_lam && !(lam >= 0.0)) return fail(BMC_ERR_INVALID, "schur step: damping %g", lam);
     const cudaStream_t st = (cudaStream_t)stream;
     double* Y = d_work;
     double* w = Y + (size_t)n_voxels * n_local;
     double* red = w + (size_t)n_voxels * n_local;
     schur_eliminate_kernel<<<(n_voxels + 127) / 128, 128, 0, st>>>(n_voxels, n_local, n_shared, d_H, d_g, d_free, lam,
-                                                                   Y, w, red);
+                                                                   d_lam, Y, w, red);
     CUDA_TRY(cudaGetLastError());
     schur_sum_kernel<<<1, 1024, 0, st>>>(n_voxels, red, d_sums);
     CUDA_TRY(cudaGetLastError());
@@ -886,16 +927,17 @@ bmc_status bmc_schur_eliminate(int32_t n_voxels, int32_t n_local, int32_t n_shar
 }
 
 bmc_status bmc_schur_back(int32_t n_voxels, int32_t n_local, int32_t n_shared, const double* d_sums, double lam,
-                          const double* d_work, double* d_dx_local, double* d_dx_shared, void* stream) {
+                          const double* d_lam, const double* d_work, double* d_dx_local, double* d_dx_shared,
+                          void* stream) {
     if (n_voxels < 1 || n_local < 1 || n_local > kMaxJointP - 1 || (n_shared != 0 && n_shared != 1))
         return fail(BMC_ERR_INVALID, "schur step: %d voxels, %d local (1..%d) and %d shared (0 or 1) values",
                     n_voxels, n_local, kMaxJointP - 1, n_shared);
     if (!d_sums || !d_work || !d_dx_local || !d_dx_shared) return fail(BMC_ERR_INVALID, "schur step: null pointer");
-    if (!(lam >= 0.0)) return fail(BMC_ERR_INVALID, "schur step: damping %g", lam);
+    if (!d_lam && !(lam >= 0.0)) return fail(BMC_ERR_INVALID, "schur step: damping %g", lam);
     const cudaStream_t st = (cudaStream_t)stream;
     const double* Y = d_work;
     const double* w = Y + (size_t)n_voxels * n_local;
-    schur_shared_kernel<<<1, 32, 0, st>>>(n_shared, d_sums, lam, d_dx_shared);
+    schur_shared_kernel<<<1, 32, 0, st>>>(n_shared, d_sums, lam, d_lam, d_dx_shared);
     CUDA_TRY(cudaGetLastError());
     const long long n = (long long)n_voxels * n_local;
     schur_back_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(n_voxels, n_local, Y, w, d_dx_shared, d_dx_local);
@@ -936,6 +978,7 @@ namespace {
 
 constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;     // 32 MiB per GPU
 constexpr size_t kNoAllocStatusBytes = 256;
+size_t noalloc_seg_bytes(long long n_rows) { return align256(sizeof(int4) * (size_t)n_rows); }
 constexpr int kNoAllocMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
@@ -987,9 +1030,16 @@ struct NoAlloc {
         a.params = params; a.m0 = m0; a.out = out;
         a.status = static_cast<int*>(scratch);
         CUDA_TRY(cudaMemsetAsync(a.status, 0, sizeof(int), st));          // must start at zero each call
-        EvRec<R>* rec = reinterpret_cast<EvRec<R>*>(static_cast<char*>(scratch) + kNoAllocStatusBytes);
+        // the scratch: the status word, every row's repeated block, the event records
+        int4* seg = reinterpret_cast<int4*>(static_cast<char*>(scratch) + kNoAllocStatusBytes);
+        EvRec<R>* rec = reinterpret_cast<EvRec<R>*>(static_cast<char*>(scratch) + kNoAllocStatusBytes +
+                                                    noalloc_seg_bytes(pr->n_offsets));
         if ((s = prep_events<R>(pr, ev, rec, st)) != BMC_OK) return s;   // overwrites the previous call's
         a.ev = rec;
+        if constexpr (std::is_same<R, double>::value) {
+            if ((s = scan_blocks(rec, pr->n_offsets, pr->n_events, pr->n_offsets, seg, st)) != BMC_OK) return s;
+            a.seg = seg;
+        }
         return launch_chain<NC, R, 0>(a, tt, st);
     }
 
@@ -1011,7 +1061,8 @@ extern "C" bmc_status bmc_simulate_noalloc(const bmc_problem* prob, const double
     if (!d_out) return fail(BMC_ERR_INVALID, "null output");
     const size_t rec_bytes = prob->precision == BMC_F32 ? sizeof(EvRec<float>) : sizeof(EvRec<double>);
     const size_t nrec = (size_t)prob->n_offsets * (size_t)prob->n_events;
-    const size_t cap = (kNoAllocScratchBytes - kNoAllocStatusBytes) / rec_bytes;
+    const size_t fixed = kNoAllocStatusBytes + noalloc_seg_bytes(prob->n_offsets);
+    const size_t cap = fixed < kNoAllocScratchBytes ? (kNoAllocScratchBytes - fixed) / rec_bytes : 0;
     if (nrec > cap)
         return fail(BMC_ERR_INVALID,
                     "bmc_simulate_noalloc: the event table (%d offsets x %d events = %zu records of %zu bytes) "

@@ -65,6 +65,10 @@ struct ChainArgs {
     const long long* tab_base; // [n_tables]: first record of each table in `ev`
     const int* tab_noff;       // [n_tables]: rows (records per event) of each table
     const int* tab_nev;        // [n_tables]: events of each table
+    // repeated blocks (propagator reuse): per row (a, L, r, 0), the r copies of the L events from event a
+    // on are applied as one propagator; r < 2: none. Uniform tables: row o; uneven: tab_row0[t] + o.
+    const int4* seg;           // null: no reuse
+    const int* tab_row0;       // [n_tables]: first row of each table in `seg` (uneven batches)
 };
 
 template <int NC>

@@ -134,7 +134,9 @@ __host__ __device__ inline void solve2(double (&A)[kMaxJointP - 1][kMaxJointP - 
 // free[v][j] (1 free, 0 held) for the local values. Writes w = A^-1 g_p and Y = A^-1 h_ps (Y zero when
 // S = 0) and the sample's terms of the shared Schur complement: red = (h_ss, h_ps^T Y, h_ps^T w, g_s).
 __host__ __device__ inline void schur_eliminate_one(int v, int n_vox, int PL, int S, const double* H, const double* g,
-                                                   const double* free, double lam, double* Y, double* w, double* red) {
+                                                   const double* free, double lam_in, const double* d_lam,
+                                                   double* Y, double* w, double* red) {
+    const double lam = d_lam ? *d_lam : lam_in;
     constexpr int M = kMaxJointP - 1;
     const int P = PL + S;
     const double* Hv = H + (size_t)v * P * P;
@@ -172,9 +174,10 @@ __host__ __device__ inline void schur_eliminate_one(int v, int n_vox, int PL, in
 
 __global__ void schur_eliminate_kernel(int n_vox, int PL, int S, const double* __restrict__ H,
                                        const double* __restrict__ g, const double* __restrict__ free, double lam,
+                                       const double* __restrict__ d_lam,
                                        double* __restrict__ Y, double* __restrict__ w, double* __restrict__ red) {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v < n_vox) schur_eliminate_one(v, n_vox, PL, S, H, g, free, lam, Y, w, red);
+    if (v < n_vox) schur_eliminate_one(v, n_vox, PL, S, H, g, free, lam, d_lam, Y, w, red);
 }
 
 // one block: the four Schur sums of a batch -- sum h_ss, sum h_ps^T Y, sum h_ps^T w, sum g_s -- in a
@@ -198,7 +201,9 @@ __global__ void schur_sum_kernel(int n_vox, const double* __restrict__ red, doub
 }
 
 // the shared step ds = -(sum g_s - sum h_ps^T w) / (H_ss + lam (H_ss + 1e-9) - sum h_ps^T Y), H_ss = sum h_ss
-__global__ void schur_shared_kernel(int S, const double* __restrict__ sums, double lam, double* __restrict__ ds) {
+__global__ void schur_shared_kernel(int S, const double* __restrict__ sums, double lam_in,
+                                    const double* __restrict__ d_lam, double* __restrict__ ds) {
+    const double lam = d_lam ? *d_lam : lam_in;
     if (threadIdx.x == 0) {
         const double hss = sums[0], sy = sums[1], tw = sums[2], gs = sums[3];
         ds[0] = S ? -(gs - tw) / (hss + lam * (hss + 1e-9) - sy) : 0.0;

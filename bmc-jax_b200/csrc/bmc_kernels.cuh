@@ -23,6 +23,10 @@ __device__ __forceinline__ R warp_max(R x) {
 // exp(X / 2^s) by a degree-m Horner recurrence (each column by the sparse operator, in registers),
 // then s squarings through shared memory, then the matrix-vector product with [M; 1].
 // lanes per chain in the dense path: one column per lane, so a warp works on 32 / group chains at once
+// the norm above which an event inside a repeated block is exponentiated densely (a short event acts on
+// the block propagator's columns by the truncated Taylor series instead)
+constexpr double kBlockDenseNorm = 4.0;
+
 template <int NC>
 struct DenseGroup {
     static constexpr int NA = Layout<NC>::NA;
@@ -43,6 +47,8 @@ struct DenseSlotBody {
     D vec[NA];                      // the owner's [M; 1]
     D out[NA];
     int s;
+    int ns, m, kind, r;             // repeated blocks: the event's Taylor sub-steps and degree, its kind
+                                    // (bit 0 dense, bit 1 Taylor, bit 2 spoil), the block's repeats
 };
 
 // A warp's G slots are read together (each group reads the same element of its own slot), so they are
@@ -111,6 +117,52 @@ struct Dense {
             if (q == j) C::at(col, q) = dconst<R, NT>(R(1));
     }
 
+    // Column gl of exp(X) into `col`, X the slot's coefficients and constant column (already scaled by
+    // dt / 2^s): the degree-m Horner recurrence T = I + X T / k, k = m .. 1, then s squarings through the
+    // slot's matrix (column j of T T is sum_l T[:, l] T[l][j]). Every lane of the warp calls it (the
+    // squarings synchronise the warp, up to the warp's largest count smax); lanes with `work` compute.
+    static __device__ __forceinline__ void exp_column(SL* sl, int gl, bool work, int s, int smax, State<NC, D>& col,
+                                                      const TaylorTable& tt) {
+        const R caug = (gl == N) ? R(1) : R(0);
+        unit(col, gl);
+        if (work) {
+            for (int k = tt.dense_m; k >= 1; --k) {
+                State<NC, D> y;
+                matvec_aug(sl, col, caug, y);
+                C::scal_state(y, R(tt.inv_k[k]));
+                State<NC, D> e;
+                unit(e, gl);
+                C::axpy_state(e, y);
+                col = e;
+            }
+        }
+        for (int q = 0; q < smax; ++q) {
+            const bool sq = work && q < s;
+            if (sq) {
+#pragma unroll
+                for (int i = 0; i < N; ++i) sl->mat[gl * LD + i] = C::at(col, i);
+                sl->mat[gl * LD + N] = dconst<R, NT>(caug);
+            }
+            __syncwarp();
+            if (sq) {
+                State<NC, D> nc;
+                unit(nc, -1);
+#pragma unroll
+                for (int l = 0; l < N; ++l) {
+                    const D w = C::at(col, l);
+#pragma unroll
+                    for (int i = 0; i < N; ++i) C::at(nc, i) = dfma(sl->mat[l * LD + i], w, C::at(nc, i));
+                }
+                if (caug != R(0)) {           // the augmented column also picks up T[:, aug]
+#pragma unroll
+                    for (int i = 0; i < N; ++i) C::at(nc, i) = C::at(nc, i) + sl->mat[N * LD + i];
+                }
+                col = nc;
+            }
+            __syncwarp();
+        }
+    }
+
     // Every lane whose `evolve` is set gets its state advanced by exp(X) [M; 1]. The warp takes up to
     // G of those chains at a time: chain g of a round is done by lanes g GS .. g GS + NA - 1, lane
     // g GS + j owning column j.
@@ -162,46 +214,7 @@ struct Dense {
             const int s = grp_owner >= 0 ? sl->s : 0;
             const int smax = (int)__reduce_max_sync(kFull, (unsigned)s);
             State<NC, D> col;
-            const R caug = (gl == N) ? R(1) : R(0);
-            // Horner: T = I + X T / k, k = m .. 1  (column gl)
-            unit(col, gl);
-            if (work) {
-                for (int k = tt.dense_m; k >= 1; --k) {
-                    State<NC, D> y;
-                    matvec_aug(sl, col, caug, y);
-                    C::scal_state(y, R(tt.inv_k[k]));
-                    State<NC, D> e;
-                    unit(e, gl);
-                    C::axpy_state(e, y);
-                    col = e;
-                }
-            }
-            // s squarings: column j of T T is sum_l T[:, l] T[l][j]
-            for (int q = 0; q < smax; ++q) {
-                const bool sq = work && q < s;
-                if (sq) {
-#pragma unroll
-                    for (int i = 0; i < N; ++i) sl->mat[gl * LD + i] = C::at(col, i);
-                    sl->mat[gl * LD + N] = dconst<R, NT>(caug);
-                }
-                __syncwarp();
-                if (sq) {
-                    State<NC, D> nc;
-                    unit(nc, -1);
-#pragma unroll
-                    for (int l = 0; l < N; ++l) {
-                        const D w = C::at(col, l);
-#pragma unroll
-                        for (int i = 0; i < N; ++i) C::at(nc, i) = dfma(sl->mat[l * LD + i], w, C::at(nc, i));
-                    }
-                    if (caug != R(0)) {           // the augmented column also picks up T[:, aug]
-#pragma unroll
-                        for (int i = 0; i < N; ++i) C::at(nc, i) = C::at(nc, i) + sl->mat[N * LD + i];
-                    }
-                    col = nc;
-                }
-                __syncwarp();
-            }
+            exp_column(sl, gl, work, s, smax, col, tt);
             // M <- T [M; 1]
             if (work) {
 #pragma unroll
@@ -218,6 +231,180 @@ struct Dense {
 #pragma unroll
                 for (int q = 0; q < N; ++q)
                     C::at(M, q) = capped ? dconst<R, NT>(R(NAN)) : sm->slot[my_slot].out[q];
+            }
+            __syncwarp();
+        }
+    }
+
+    // Propagator reuse for a repeated block of events. Every lane whose `start` is set advances its state
+    // through r repeats of the L events of its own row that begin at event `first` (records
+    // row[e * stride]): its group builds the block's augmented propagator P = E_L ... E_1 one event at a
+    // time, lane j holding column j of P -- an event of norm above kBlockDenseNorm is exponentiated densely
+    // (exp_column) and multiplied in, a shorter one acts on every column by the truncated Taylor series
+    // (the degree and sub-steps of the table's tolerance), a spoiler or gradient zeroes the transverse
+    // rows -- and then applies P r times to [M; 1]. Each chain uses only its own row and parameters, so
+    // its result does not depend on the chains that share its warp. The work counts follow the dense
+    // path's units: Horner column products, squarings (one more per dense event for the product with P)
+    // and Taylor terms (every column's, plus one per application of P).
+    static __device__ __noinline__ void block(SM* sm, int lane, bool start, const EvRec<R>* row, int stride,
+                                              int first, int L, int r, const ChainConst<NC, D>& cc,
+                                              State<NC, D>& M, const TaylorTable& tt, int* status, bool count,
+                                              unsigned& wt, unsigned& wh, unsigned& ws) {
+        const int grp = lane / GS, gl = lane % GS;
+        const R thm = R(tt.theta[tt.m_max]);
+        unsigned need = __ballot_sync(kFull, start);
+        while (need) {
+            int my_slot = -1, grp_owner = -1;
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+                const int c = need ? __ffs(need) - 1 : -1;
+                if (need) need &= need - 1;
+                if (c == lane) my_slot = g;
+                if (g == grp) grp_owner = c;
+            }
+            bool capped = false;
+            const int Lw = (int)__reduce_max_sync(kFull, (unsigned)(my_slot >= 0 ? L : 0));
+            const int rw = (int)__reduce_max_sync(kFull, (unsigned)(my_slot >= 0 ? r : 0));
+            SL* sl = &sm->slot[grp];
+            const bool work = grp_owner >= 0 && gl < NA;
+            const R pa = (gl == N) ? R(1) : R(0);          // P's augmented row entry in this column
+            State<NC, D> P;
+            unit(P, gl);
+            for (int k = 0; k < Lw; ++k) {
+                if (my_slot >= 0) {                          // the owner prepares its event k
+                    SL* so = &sm->slot[my_slot];
+                    int kind = 0;
+                    if (k < L) {
+                        const EvRec<R> rec = row[(size_t)(first + k) * stride];
+                        if (rec.dt > R(1e-9)) {
+                            D g = dconst<R, NT>(R(0));
+                            if (cc.mt_on && cc.ls != 0 && rec.w1 != R(0)) {
+                                const D offmt = (rec.wf - cc.dw0) - cc.dwmt;
+                                g = cc.ls == 1 ? lorentzian<R, NT>(offmt, cc.t2mt)
+                                               : super_lorentzian<R, NT>(offmt, cc.t2mt, cc.w0sl);
+                            }
+                            StepCoef<NC, D> sc;
+                            C::event_coef(cc, rec, g, sc);
+                            R nu = rec.dt * C::coef_norm(sc, cc);
+                            if (!(nu < R(INFINITY))) {
+                                atomicOr(status, 1);
+                                nu = R(0);
+                            }
+                            R h;
+                            if (nu > R(kBlockDenseNorm)) {
+                                int s = (int)ceil(log2(double(nu) / tt.dense_theta));
+                                if (s > 200) {
+                                    s = 200;
+                                    capped = true;
+                                    atomicOr(status, 2);
+                                }
+                                so->s = s;
+                                h = R(ldexp(double(rec.dt), -s));
+                                kind = 1;
+                                if (count) {
+                                    wh += unsigned(NA * tt.dense_m);
+                                    ws += unsigned(s + 1);
+                                }
+                            } else {
+                                const int ns = nu > thm ? (int)ceil(nu / thm) : 1;
+                                const R per = ns == 1 ? nu : nu / R(ns);
+                                int m = 1;
+                                while (m < tt.m_max && R(tt.theta[m]) < per) ++m;
+                                so->s = 0;
+                                so->ns = ns;
+                                so->m = m;
+                                h = ns == 1 ? rec.dt : rec.dt / R(ns);
+                                kind = 2;
+                                if (count) wt += unsigned(NA * ns * m);
+                            }
+                            C::scale_coef(sc, h);
+                            so->coef = sc;
+                            so->cw = dconst<R, NT>(h) * cc.cw;
+                            so->cm = dconst<R, NT>(h) * cc.cm;
+#pragma unroll
+                            for (int i = 0; i < NC; ++i) so->cc[i] = dconst<R, NT>(h) * cc.cc[i];
+                        }
+                        const int type = (int)rec.type;
+                        if (type == EV_GRADIENT || type == EV_SPOILER) kind |= 4;
+                    }
+                    so->kind = kind;
+                }
+                __syncwarp();
+                const int kd = grp_owner >= 0 ? sl->kind : 0;
+                const bool dense = work && (kd & 1);
+                if (__any_sync(kFull, dense)) {
+                    const int s = dense ? sl->s : 0;
+                    const int smax = (int)__reduce_max_sync(kFull, (unsigned)s);
+                    State<NC, D> T;
+                    exp_column(sl, gl, dense, s, smax, T, tt);
+                    if (dense) {
+#pragma unroll
+                        for (int i = 0; i < N; ++i) sl->mat[gl * LD + i] = C::at(T, i);
+                    }
+                    __syncwarp();
+                    if (dense) {                             // column gl of T [P; pa]
+                        State<NC, D> np;
+                        unit(np, -1);
+#pragma unroll
+                        for (int l = 0; l < N; ++l) {
+                            const D w = C::at(P, l);
+#pragma unroll
+                            for (int i = 0; i < N; ++i) C::at(np, i) = dfma(sl->mat[l * LD + i], w, C::at(np, i));
+                        }
+                        if (pa != R(0)) {
+#pragma unroll
+                            for (int i = 0; i < N; ++i) C::at(np, i) = C::at(np, i) + sl->mat[N * LD + i];
+                        }
+                        P = np;
+                    }
+                }
+                if (work && (kd & 2)) {                      // P <- exp(X)^ns P, column by column
+                    const int ns = sl->ns, m = sl->m;
+                    for (int j = 0; j < ns; ++j) {
+                        State<NC, D> term = P;
+                        R ca = pa;
+                        for (int q = 1; q <= m; ++q) {
+                            State<NC, D> y;
+                            matvec_aug(sl, term, ca, y);
+                            C::scal_state(y, R(tt.inv_k[q]));
+                            term = y;
+                            ca = R(0);
+                            C::axpy_state(P, term);
+                        }
+                    }
+                }
+                if (work && (kd & 4)) C::spoil(P);
+                __syncwarp();
+            }
+            // M <- P^r [M; 1]
+            if (work) {
+#pragma unroll
+                for (int i = 0; i < N; ++i) sl->mat[gl * LD + i] = C::at(P, i);
+            }
+            if (my_slot >= 0) {
+                SL* so = &sm->slot[my_slot];
+#pragma unroll
+                for (int q = 0; q < N; ++q) so->vec[q] = C::at(M, q);
+                so->vec[N] = dconst<R, NT>(R(1));
+                so->r = r;
+                if (count) wt += unsigned(r);
+            }
+            __syncwarp();
+            const int rr = grp_owner >= 0 ? sl->r : 0;
+            for (int q = 0; q < rw; ++q) {
+                const bool app = grp_owner >= 0 && gl < N && q < rr;
+                D acc = dconst<R, NT>(R(0));
+                if (app) {
+                    for (int j = 0; j < NA; ++j) acc = dfma(sl->mat[j * LD + gl], sl->vec[j], acc);
+                }
+                __syncwarp();
+                if (app) sl->vec[gl] = acc;
+                __syncwarp();
+            }
+            if (my_slot >= 0) {
+#pragma unroll
+                for (int q = 0; q < N; ++q)
+                    C::at(M, q) = capped ? dconst<R, NT>(R(NAN)) : sm->slot[my_slot].vec[q];
             }
             __syncwarp();
         }
@@ -270,6 +457,7 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
     int v, o;
     const EvRec<R>* __restrict__ ev = reinterpret_cast<const EvRec<R>*>(a.ev);
     int stride = a.n_off, n_ev_own = a.n_ev, n_ev_loop = a.n_ev;
+    int seg_row;
     if constexpr (UNEVEN) {
         // this chain's table: its records, row stride and length; the warp runs to its longest table
         const int2 vm = a.chain_map[ci];
@@ -280,10 +468,19 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
         stride = a.tab_noff[t];
         n_ev_own = a.tab_nev[t];
         n_ev_loop = (int)__reduce_max_sync(kFull, (unsigned)n_ev_own);
+        seg_row = a.tab_row0 ? a.tab_row0[t] + o : 0;
     } else {
         v = (int)(ci / a.n_off);
         o = (int)(ci % a.n_off);
+        seg_row = o;
     }
+    // this chain's repeated block (float64 kernels; not with a trajectory, whose every event is kept)
+    int4 blk = make_int4(0, 0, 0, 0);
+    if constexpr (std::is_same<R, RD>::value) {
+        if (a.seg && !a.traj) blk = a.seg[seg_row];
+    }
+    const bool use_blk = blk.z >= 2;
+    const int blk_end = use_blk ? blk.x + blk.z * blk.y : 0;
     const bool act = valid && (a.active == nullptr || a.active[v] != 0);
     if (__all_sync(kFull, !act)) return;
 
@@ -324,8 +521,16 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
                 C::load_m0(a, v, M);
                 reset_pending = false;
             }
-            const int type = (int)rec.type;
-            const bool evolve = act && rec.dt > R(1e-9);
+            // a repeated block: all its events at once at its first event, none of them afterwards
+            if constexpr (std::is_same<R, RD>::value) {
+                const bool bstart = use_blk && act && in && e == blk.x;
+                if (__any_sync(kFull, bstart))
+                    Dense<NC, R, NT>::block(dsm, lane, bstart, ev + o, stride, blk.x, blk.y, blk.z, cc, M, tt, a.status,
+                                            count, wk0, wk1, wk2);
+            }
+            const bool skip = use_blk && e >= blk.x && e < blk_end;
+            const int type = skip ? EV_DELAY : (int)rec.type;
+            const bool evolve = act && !skip && rec.dt > R(1e-9);
             if (__any_sync(kFull, evolve)) {
                 D g = dconst<R, NT>(R(0));
                 if (mt_ls && rec.w1 != R(0)) {
@@ -485,6 +690,63 @@ __global__ void __launch_bounds__(128) cost_kernel(const ChainArgs a, float* __r
     }
     key[ci] = cost;
     idx[ci] = (int)ci;
+}
+
+// ------------------------------------------------------------------------------------------------
+// repeated blocks: for every row of a table, the run of r >= 2 identical copies of a block of
+// L <= kBlockMaxL events that saves the most events, among the blocks that hold no readout, evolve the
+// state, and either hold an event of at least kBlockMinDt (exponentiated densely, the work the reuse
+// saves) or repeat so often (r >= kBlockMinRepeats) that the per-column work of short events pays;
+// (0, 0, 0) where there is none. One thread per row.
+// ------------------------------------------------------------------------------------------------
+constexpr int kBlockMaxL = 8;
+constexpr double kBlockMinDt = 1e-3;
+constexpr int kBlockMinRepeats = 48;
+
+template <typename R>
+__device__ __forceinline__ bool same_rec(const EvRec<R>& x, const EvRec<R>& y) {
+    return x.dt == y.dt && x.w1 == y.w1 && x.c == y.c && x.s == y.s && x.wf == y.wf && x.type == y.type;
+}
+
+template <typename R>
+__global__ void block_scan_kernel(const EvRec<R>* __restrict__ ev, int n_rows, int n_ev, int stride,
+                                  int4* __restrict__ seg) {
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n_rows) return;
+    const EvRec<R>* row = ev + o;
+    int4 best = make_int4(0, 0, 0, 0);
+    long long best_save = 0;
+    for (int L = 1; L <= kBlockMaxL; ++L) {
+        int a = 0;
+        while (a + 2 * L <= n_ev) {
+            int r = 1;
+            while (a + (r + 1) * L <= n_ev) {
+                bool eq = true;
+                for (int j = 0; j < L && eq; ++j)
+                    eq = same_rec(row[(size_t)(a + j) * stride], row[(size_t)(a + r * L + j) * stride]);
+                if (!eq) break;
+                ++r;
+            }
+            if (r < 2) {
+                ++a;
+                continue;
+            }
+            bool adc = false, moves = false, long_ev = false;
+            for (int j = 0; j < L; ++j) {
+                const EvRec<R> x = row[(size_t)(a + j) * stride];
+                adc |= (int)x.type == EV_ADC;
+                moves |= x.dt > R(1e-9);
+                long_ev |= x.dt >= R(kBlockMinDt);
+            }
+            const long long save = (long long)(r - 1) * L;
+            if (!adc && moves && (long_ev || r >= kBlockMinRepeats) && save > best_save) {
+                best = make_int4(a, L, r, 0);
+                best_save = save;
+            }
+            a += r * L;
+        }
+    }
+    seg[o] = best;
 }
 
 // ------------------------------------------------------------------------------------------------

@@ -223,8 +223,10 @@ bmc_status bmc_simulate_noalloc(const bmc_problem* prob, const double* d_params,
  *   bmc_uneven_simulate: d_params [13 + 5 n_cest][n_voxels], d_m0 [n_voxels][N], an optional B0 spread
  *     (as for bmc_simulate, sigma per voxel); d_z [n_chains] = state mz_loc after each chain's last
  *     event; with tangents (field rows -1..n_fields-1, and BMC_SEED_SPREAD_SIGMA with a spread),
- *     d_jz [n_tangents][n_chains]. Replaces simulation/simulate.py:134-148 + voxels.py:89-129 +
- *     spread.py:77-106 per shape class, and the jacfwd of fitting/joint.py:300,317.
+ *     d_jz [n_tangents][n_chains]. d_active [n_voxels] (device, may be NULL = all): voxels with 0 are
+ *     skipped and their outputs left as they were (a fit re-launches only what moved, with no host
+ *     synchronisation). Replaces simulation/simulate.py:134-148 + voxels.py:89-129 + spread.py:77-106 per
+ *     shape class, and the jacfwd of fitting/joint.py:300,317.
  */
 typedef struct {
     int32_t n_tables;
@@ -237,8 +239,8 @@ bmc_status bmc_uneven_create(int32_t n_cest, int32_t n_voxels, const int32_t* h_
                              const bmc_table_set* tables, int32_t mz_loc, int32_t reset_after_adc, void** plan,
                              int64_t* n_chains, int64_t* h_chain_start);
 bmc_status bmc_uneven_simulate(const void* plan, const double* d_params, const double* d_m0,
-                               const bmc_spread* spread, const bmc_tangents* tangents, double* d_z, double* d_jz,
-                               void* stream);
+                               const bmc_spread* spread, const bmc_tangents* tangents, const int32_t* d_active,
+                               double* d_z, double* d_jz, void* stream);
 bmc_status bmc_uneven_destroy(void* plan);
 
 /*
@@ -247,6 +249,8 @@ bmc_status bmc_uneven_destroy(void* plan);
  *   bmc_normal_segments: per voxel v, over its chains d_chain_start[v] .. d_chain_start[v+1]-1:
  *     d_H [n_voxels][P][P] = J J^T, d_g [n_voxels][P] = J r, d_c [n_voxels] = r^T r, with
  *     d_jz [P][n_chains] and d_r [n_chains]; P <= 9.
+ *   The damping is `lam`, or *d_lam when d_lam (device, one double) is not NULL: a loop that keeps lambda
+ *   on the device then needs no host synchronisation.
  *   bmc_schur_step: P = n_local + n_shared (the shared column last, n_shared 0 or 1, n_local <= 8);
  *     d_free [n_voxels][n_local] (1 free, 0 held; NULL = all free) -> d_dx_local [n_voxels][n_local],
  *     d_dx_shared [1]. d_work holds (2 n_local + 4) n_voxels + 4 doubles. The shared sums are taken in
@@ -260,13 +264,14 @@ bmc_status bmc_normal_segments(int32_t n_voxels, int32_t n_params, int64_t n_cha
                                const double* d_jz, const double* d_r, double* d_H, double* d_g, double* d_c,
                                void* stream);
 bmc_status bmc_schur_step(int32_t n_voxels, int32_t n_local, int32_t n_shared, const double* d_H, const double* d_g,
-                          const double* d_free, double lam, double* d_dx_local, double* d_dx_shared, double* d_work,
-                          void* stream);
+                          const double* d_free, double lam, const double* d_lam, double* d_dx_local,
+                          double* d_dx_shared, double* d_work, void* stream);
 bmc_status bmc_schur_eliminate(int32_t n_voxels, int32_t n_local, int32_t n_shared, const double* d_H,
-                               const double* d_g, const double* d_free, double lam, double* d_work, double* d_sums,
-                               void* stream);
+                               const double* d_g, const double* d_free, double lam, const double* d_lam,
+                               double* d_work, double* d_sums, void* stream);
 bmc_status bmc_schur_back(int32_t n_voxels, int32_t n_local, int32_t n_shared, const double* d_sums, double lam,
-                          const double* d_work, double* d_dx_local, double* d_dx_shared, void* stream);
+                          const double* d_lam, const double* d_work, double* d_dx_local, double* d_dx_shared,
+                          void* stream);
 
 /*
  * Learned warm start: a multilayer perceptron that maps a measured saturation ladder to normalised

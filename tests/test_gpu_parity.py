@@ -178,6 +178,61 @@ def test_stacking_is_bit_exact_with_mixed_taylor_degrees(cuda):
         np.testing.assert_array_equal(zr[i * 23:(i + 1) * 23], z)
 
 
+def _block_train(n_off, n_pulses, ppm_lo=-6.0, ppm_hi=6.0, tp=0.05, gap=0.005, b1=2.0, b0=3.0, rec=1.0):
+    """Block-pulse saturation (one RF event per pulse, as the uneven configuration's trains): a recovery,
+    n_pulses x (tp RF block, gap), spoiler, ADC."""
+    T, DT, A = [0], [rec], [0.0]
+    for _ in range(n_pulses):
+        T += [1, 0]; DT += [tp, gap]; A += [b1 * 267.5153 / (2 * np.pi), 0.0]
+    T += [4, 3]; DT += [0.0, 0.0]; A += [0.0, 0.0]
+    ne = len(T)
+    freq = np.linspace(ppm_lo, ppm_hi, n_off) * 42.5764 * b0
+    rf = np.where(np.array(T)[None, :] == 1, freq[:, None], 0.0)
+    return O.Events(np.tile(np.int32(T), (n_off, 1)), np.tile(np.float64(DT), (n_off, 1)),
+                    np.tile(np.float64(A), (n_off, 1)), np.zeros((n_off, ne)), rf,
+                    np.tile(np.int32([-1] * (ne - 1) + [0]), (n_off, 1)))
+
+
+@pytest.mark.parametrize("nc,n_pulses", [(1, 7), (4, 12), (5, 3)])
+def test_repeated_block_pulses_match_the_oracle(cuda, nc, n_pulses):
+    """A train of identical 50 ms block pulses: the kernel applies the propagator of one (pulse, gap) block
+    n_pulses times (propagator reuse); Z and its tangents against the oracle's event-by-event expm."""
+    from bmc_b200.design import jacobian
+    from bmc_b200.fitting import Experiment, FitSpec, FreeParam
+    from bmc_b200.simulation import SimParams, SimEvent, simulate_z
+    pb = _random_batch(4, nc, seed=20 + nc)
+    ev = _block_train(9, n_pulses)
+    mz = O.mz_loc(nc)
+    m0 = np.stack([O.initial_state(O.sample(pb, i)) for i in range(4)])
+    z = simulate_z(SimParams(*pb), SimEvent(*ev), m0, mz)
+    want = np.stack([O.simulate_spectrum(O.sample(pb, i), ev, m0[i])[:, mz] for i in range(4)])
+    np.testing.assert_allclose(z, want, rtol=0, atol=1e-10)
+    p1 = O.sample(pb, 1)
+    field = "cest_k" if nc else "water_r2"
+    x = float(np.atleast_1d(getattr(p1, field))[0])
+    spec = FitSpec([FreeParam("a", field, 0 if nc else None, 1.0, 0.0, 1e9, x)])
+    Z, J = jacobian(Experiment(SimParams(*p1), SimEvent(*ev), m0[1], mz), spec, [x])
+    Zo, Jo = O.spectrum_jacobian(p1, ev, m0[1], [O.Slot(field, 0 if nc else None)])
+    np.testing.assert_allclose(Z, Zo, rtol=0, atol=1e-10)
+    np.testing.assert_allclose(J, Jo, rtol=1e-7, atol=1e-9 * max(1.0, np.abs(Jo).max()))
+
+
+def test_stacking_is_bit_exact_with_repeated_blocks(cuda):
+    """Stacked block-pulse trains of different lengths (front-padded to the longest): each row's repeated
+    block is found at its own place and applied the same way as in the row's own experiment."""
+    from bmc_b200.fitting import Experiment
+    from bmc_b200.simulation import SimParams, SimEvent
+    pb = _random_batch(1, 4, seed=9, mt=True)
+    p1 = SimParams(*O.sample(pb, 0))
+    m0 = O.initial_state(O.sample(pb, 0))
+    parts = [Experiment(p1, SimEvent(*_block_train(17, n, ppm_lo=-5.0 + i)), m0, O.mz_loc(4))
+             for i, n in enumerate((3, 8, 5))]
+    alone = [part.simulate() for part in parts]
+    zj = Experiment.stack(parts).simulate()
+    for i, z in enumerate(alone):
+        np.testing.assert_array_equal(zj[i * 17:(i + 1) * 17], z)
+
+
 def test_jacobian_matches_the_oracle_and_the_reference(cuda):
     from bmc_b200.design import jacobian
     from bmc_b200.fitting import Experiment, FitSpec, FreeParam

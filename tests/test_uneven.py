@@ -134,6 +134,20 @@ def test_joint_fit_follows_the_dense_oracle_lm(mixed):
     assert res.shared == pytest.approx(xo[-1] * scl[4], rel=1e-6)
 
 
+def test_joint_fit_from_a_cuda_graph_equals_the_eager_loop(mixed):
+    """One iteration captured in a CUDA graph and replayed gives the eager loop's iterates bit for bit."""
+    from bmc_b200.simulation import simulate_z
+    from bmc_b200.uneven import UnevenBatch, fit_joint_uneven
+    exps = mixed[:9]
+    z = [simulate_z(e.params, e.events, e.m0, e.mz_loc) + 0.001 * np.cos(np.arange(np.shape(e.events.dt)[0]))
+         for e in exps]
+    a = fit_joint_uneven(UnevenBatch(exps), _spec(), z, n_iter=7, graph=True)
+    b = fit_joint_uneven(UnevenBatch(exps), _spec(), z, n_iter=7, graph=False)
+    np.testing.assert_array_equal(a.x, b.x)
+    np.testing.assert_array_equal(a.cost, b.cost)
+    assert a.shared == b.shared
+
+
 def test_joint_fit_recovers_the_truth(mixed):
     from bmc_b200.simulation import simulate_z
     from bmc_b200.uneven import UnevenBatch, fit_joint_uneven
@@ -167,23 +181,24 @@ def test_schur_step_in_one_call_and_in_shards_is_the_dense_step(cuda):
     d = torch.empty((n, PL), dtype=torch.float64, device="cuda")
     ds = torch.empty(1, dtype=torch.float64, device="cuda")
     work = torch.empty((2 * PL + 4) * n + 4, dtype=torch.float64, device="cuda")
-    _lib.check(L.bmc_schur_step(n, PL, 1, _lib.ptr(dH), _lib.ptr(dg), _lib.ptr(dfree), lam, _lib.ptr(d), _lib.ptr(ds),
-                                _lib.ptr(work), _lib.stream_handle()))
+    _lib.check(L.bmc_schur_step(n, PL, 1, _lib.ptr(dH), _lib.ptr(dg), _lib.ptr(dfree), lam, None, _lib.ptr(d),
+                                _lib.ptr(ds), _lib.ptr(work), _lib.stream_handle()))
     np.testing.assert_allclose(d.cpu().numpy(), d_want, rtol=1e-10, atol=1e-12)
     assert float(ds.item()) == pytest.approx(ds_want, rel=1e-10)
-    # two shards
+    # two shards, the damping read from device memory
+    d_lam = torch.tensor([lam], dtype=torch.float64, device="cuda")
     cut = 15
     parts = [(slice(0, cut), cut), (slice(cut, n), n - cut)]
     works = [torch.empty((2 * PL + 4) * m, dtype=torch.float64, device="cuda") for _, m in parts]
     sums = [torch.empty(4, dtype=torch.float64, device="cuda") for _ in parts]
     for (sl, m), wk, sm in zip(parts, works, sums):
         _lib.check(L.bmc_schur_eliminate(m, PL, 1, _lib.ptr(dH[sl].contiguous()), _lib.ptr(dg[sl].contiguous()),
-                                         _lib.ptr(dfree[sl].contiguous()), lam, _lib.ptr(wk), _lib.ptr(sm),
-                                         _lib.stream_handle()))
+                                         _lib.ptr(dfree[sl].contiguous()), -1.0, _lib.ptr(d_lam), _lib.ptr(wk),
+                                         _lib.ptr(sm), _lib.stream_handle()))
     total = sums[0] + sums[1]
     for (sl, m), wk in zip(parts, works):
         dd = torch.empty((m, PL), dtype=torch.float64, device="cuda")
-        _lib.check(L.bmc_schur_back(m, PL, 1, _lib.ptr(total), lam, _lib.ptr(wk), _lib.ptr(dd), _lib.ptr(ds),
-                                    _lib.stream_handle()))
+        _lib.check(L.bmc_schur_back(m, PL, 1, _lib.ptr(total), -1.0, _lib.ptr(d_lam), _lib.ptr(wk), _lib.ptr(dd),
+                                    _lib.ptr(ds), _lib.stream_handle()))
         np.testing.assert_allclose(dd.cpu().numpy(), d_want[sl], rtol=1e-10, atol=1e-12)
     assert float(ds.item()) == pytest.approx(ds_want, rel=1e-10)
