@@ -820,6 +820,7 @@ def run_uneven(args, rank, world, local_rank):
                     FreeParam("r2w", "water_r2", None, 10.0, 5.0, 50.0, 1 / 0.07),
                     FreeParam("b0", "b0_inhom", None, 0.1, -0.5, 0.5, 0.0),
                     FreeParam("r1w", "water_r1", None, 1.0, 0.2, 2.0, 0.7, scope="shared")])
+    from bmc_b200.autotune import tune_dense_switch
     t0 = time.perf_counter()
     batch = UnevenBatch(exps)
     z_true = batch.simulate()
@@ -827,6 +828,9 @@ def run_uneven(args, rank, world, local_rank):
     z = [zt + 0.005 * rng.standard_normal(zt.shape) for zt in z_true]
     torch.cuda.synchronize()
     setup_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    tuning = tune_dense_switch(batch)
+    tune_s = time.perf_counter() - t0
     t0 = time.perf_counter()
     res = fit_joint_uneven(batch, spec, z, n_iter=30)
     torch.cuda.synchronize()
@@ -842,6 +846,8 @@ def run_uneven(args, rank, world, local_rank):
                                    "1..40 block pulses per row, 6 free per voxel + shared water R1, 30 iterations",
                        "voxels_per_pool_count": {int(k): int((nc == k).sum()) for k in range(1, 6)},
                        "tables": n_tables, "chains": chains, "chain_events": ev, "setup_s": setup_s,
+                       "autotune_s": tune_s,
+                       "dense_switch": {k: v["dense_switch"] for k, v in tuning.items()},
                        "shared_r1w": {"fit": res.shared, "truth": 1 / 1.3,
                                       "rel_err": abs(res.shared * 1.3 - 1.0)},
                        "rms_over_sigma_median": float(np.median(res.rms / 0.005)),

@@ -354,6 +354,7 @@ struct UnevenPlan {
     int* tab_nev = nullptr;
     int4* seg = nullptr;       // the repeated block of every row of every table
     int* tab_row0 = nullptr;   // first row of each table in seg
+    double dense_switch = 0.0; // > 0: the dense path's norm threshold for this plan (bmc_uneven_set_dense_switch)
     void* scratch = nullptr;   // sort keys and indices, cub scratch, status word
     size_t scratch_bytes = 0;
 };
@@ -377,7 +378,7 @@ struct Impl {
         a.ev = pl.rec;
         a.n_chains = pl.n_chains; a.chain_map = pl.chain_map; a.vox_table = pl.vox_table;
         a.tab_base = pl.tab_base; a.tab_noff = pl.tab_noff; a.tab_nev = pl.tab_nev;
-        a.seg = pl.seg; a.tab_row0 = pl.tab_row0; a.active = active;
+        a.seg = pl.seg; a.tab_row0 = pl.tab_row0; a.active = active; a.dense_switch = pl.dense_switch;
         Carve cv(pl.scratch);
         a.status = cv.take<int>(1);
         CUDA_TRY(cudaMemsetAsync(a.status, 0, sizeof(int), st));
@@ -860,6 +861,13 @@ bmc_status bmc_uneven_simulate(const void* plan, const double* d_params, const d
                             nf - 1);
     }
     BMC_DISPATCH(pl->n_cest, uneven(*pl, d_params, d_m0, spread, tangents, d_active, d_z, d_jz, (cudaStream_t)stream));
+}
+
+bmc_status bmc_uneven_set_dense_switch(void* plan, double norm) {
+    if (!plan) return fail(BMC_ERR_INVALID, "uneven: null plan");
+    if (!(norm >= 0.0) || norm > 1e6) return fail(BMC_ERR_INVALID, "uneven: dense-path norm %g outside 0..1e6", norm);
+    static_cast<UnevenPlan*>(plan)->dense_switch = norm;
+    return BMC_OK;
 }
 
 bmc_status bmc_uneven_destroy(void* plan) {

@@ -69,6 +69,7 @@ struct ChainArgs {
     // on are applied as one propagator; r < 2: none. Uniform tables: row o; uneven: tab_row0[t] + o.
     const int4* seg;           // null: no reuse
     const int* tab_row0;       // [n_tables]: first row of each table in `seg` (uneven batches)
+    double dense_switch;       // > 0: the norm above which an event takes the dense path (else the table's)
 };
 
 template <int NC>

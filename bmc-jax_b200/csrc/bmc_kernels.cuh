@@ -480,6 +480,7 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
         if (a.seg && !a.traj) blk = a.seg[seg_row];
     }
     const bool use_blk = blk.z >= 2;
+    const R dswitch = R(a.dense_switch > 0.0 ? a.dense_switch : tt.dense_switch);
     const int blk_end = use_blk ? blk.x + blk.z * blk.y : 0;
     const bool act = valid && (a.active == nullptr || a.active[v] != 0);
     if (__all_sync(kFull, !act)) return;
@@ -557,7 +558,7 @@ __global__ void __launch_bounds__(128, (NT == 0 ? 3 : 2)) chain_kernel(const Cha
                 }
                 // this chain's own choice: dense scaling and squaring for a large norm, else the
                 // Taylor action with the fewest terms whose tail bound meets the tolerance
-                const bool dense_own = evolve && nu > R(tt.dense_switch);
+                const bool dense_own = evolve && nu > dswitch;
                 if (__any_sync(kFull, dense_own)) {
                     StepCoef<NC, D> sc;                            // unscaled: the dense path scales by dt / 2^s
                     C::event_coef(cc, rec, g, sc);

@@ -242,6 +242,11 @@ bmc_status bmc_uneven_simulate(const void* plan, const double* d_params, const d
                                const bmc_spread* spread, const bmc_tangents* tangents, const int32_t* d_active,
                                double* d_z, double* d_jz, void* stream);
 bmc_status bmc_uneven_destroy(void* plan);
+/* The norm ||X|| = dt ||A|| above which an event of this plan's chains is exponentiated densely (one lane
+ * group per chain, scaling and squaring) rather than by the truncated Taylor action (one lane per chain);
+ * 0 restores the library's default (100). A tuning knob with no counterpart in the reference: both
+ * paths meet the same tolerance, only their speed differs (bmc_b200.autotune measures it per plan). */
+bmc_status bmc_uneven_set_dense_switch(void* plan, double norm);
 
 /*
  * The damped joint step with one value shared by every sample (fitting/joint.py:149-162's

@@ -148,6 +148,29 @@ def test_joint_fit_from_a_cuda_graph_equals_the_eager_loop(mixed):
     assert a.shared == b.shared
 
 
+def test_dense_switch_changes_the_path_not_the_result(mixed, tmp_path):
+    """The dense-path threshold of a plan (bmc_uneven_set_dense_switch) picks how an event is
+    exponentiated, not what comes out (both paths meet the tolerance); the autotuner's choices survive a
+    round trip through its JSON file."""
+    from bmc_b200 import _lib
+    from bmc_b200.autotune import apply_tuning, tune_dense_switch
+    from bmc_b200.uneven import UnevenBatch
+    batch = UnevenBatch(mixed)
+    ref = batch.simulate()
+    for norm in (8.0, 1e5):
+        for g in batch.groups:
+            _lib.check(_lib.lib().bmc_uneven_set_dense_switch(g.plan.plan, norm))
+        for a, b in zip(batch.simulate(), ref):
+            np.testing.assert_allclose(a, b, rtol=0, atol=1e-12)
+    with pytest.raises(RuntimeError, match="dense-path norm"):
+        _lib.check(_lib.lib().bmc_uneven_set_dense_switch(batch.groups[0].plan.plan, -1.0))
+    path = tmp_path / "tuning.json"
+    chosen = tune_dense_switch(batch, candidates=(25.0, 100.0), repeats=1, path=str(path))
+    assert set(chosen) == {k for k in chosen} and len(chosen) == len(batch.groups)
+    again = apply_tuning(UnevenBatch(mixed), str(path))
+    assert again == {k: v["dense_switch"] for k, v in chosen.items()}
+
+
 def test_joint_fit_recovers_the_truth(mixed):
     from bmc_b200.simulation import simulate_z
     from bmc_b200.uneven import UnevenBatch, fit_joint_uneven
