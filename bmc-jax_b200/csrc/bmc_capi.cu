@@ -103,10 +103,10 @@ TaylorTable make_table(double tol, int m_max, double dense_theta, double dense_s
 // The mixed precision's Taylor tolerance and float32 threshold (BMC_MIXED in include/bmc_b200.h); a
 // build may set others with -D for a sweep.
 #ifndef BMC_MIXED_TOL
-#define BMC_MIXED_TOL 1e-10
+#define BMC_MIXED_TOL 1e-9
 #endif
 #ifndef BMC_MIXED_F32
-#define BMC_MIXED_F32 0.3
+#define BMC_MIXED_F32 1.0
 #endif
 
 __device__ TaylorTable g_tables[3];   // [BMC_F64, BMC_F32, BMC_MIXED], per device
@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(256) fma_probe_kernel(int iters, R seed, R* si
 // ------------------------------------------------------------------------------------------------
 template <int NC, typename R, int NT, bool U = false>
 bmc_status launch_chain(const ChainArgs& a, const TaylorTable* tt, cudaStream_t st) {
-    constexpr int kWarps = 4;
+    constexpr int kWarps = ChainLaunch<NC, NT>::kWarps;
     const size_t smem = kWarps * sizeof(DenseSmem<NC, typename DenseReal<R>::type, NT>) +
                         32 * kWarps * sizeof(ChainConst<NC, Dn<R, NT>>);
     // the attribute once per device and instantiation: later calls then only enqueue work (which keeps
@@ -289,7 +289,7 @@ bmc_status launch_chain(const ChainArgs& a, const TaylorTable* tt, cudaStream_t 
         if (dev < 64) configured.fetch_or(1ull << dev, std::memory_order_acq_rel);
     }
     const long long nch = U ? a.n_chains : (long long)a.n_vox * a.n_off;
-    const long long blocks = (nch + 127) / 128;
+    const long long blocks = (nch + kWarps * 32 - 1) / (kWarps * 32);
     if (blocks > 0x7fffffffLL) return fail(BMC_ERR_INVALID, "%lld chains exceed one launch", nch);
     if (blocks == 0) return BMC_OK;
     chain_kernel<NC, R, NT, U><<<(unsigned)blocks, kWarps * 32, smem, st>>>(a, tt);
