@@ -20,7 +20,7 @@ from . import _lib
 
 __all__ = ["tune_dense_switch", "apply_tuning", "plan_key"]
 
-DEFAULT_CANDIDATES = (6.0, 12.0, 25.0, 50.0, 100.0, 200.0)
+DEFAULT_CANDIDATES = (3.0, 6.0, 12.0, 25.0, 50.0, 100.0)
 
 
 def plan_key(group) -> str:

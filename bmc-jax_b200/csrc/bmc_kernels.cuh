@@ -27,31 +27,26 @@ __device__ __forceinline__ R warp_max(R x) {
 // the block propagator's columns by the truncated Taylor series instead)
 constexpr double kBlockDenseNorm = 4.0;
 
-// Lanes per chain in the dense path: one column per lane, so a warp works on 32 / GS chains at once.
-// With four CEST pools the state has 16 entries and the augmented matrix 17 columns, one too many for
-// 16 lanes: there the augmented column is kept apart (kApart) -- its Horner recurrence computed by every
-// lane of the group, its squaring update phi' = E phi + phi spread over the lanes by rows -- so that two
-// chains share a warp.
+// lanes per chain in the dense path: one column per lane, so a warp works on 32 / GS chains at once
 template <int NC>
 struct DenseGroup {
-    static constexpr int N = Layout<NC>::N;
     static constexpr int NA = Layout<NC>::NA;
-    static constexpr bool kApart = NA > 16 && N <= 16;
-    static constexpr int W = kApart ? N : NA;      // lanes of a group that own a column
-    static constexpr int GS = W <= 8 ? 8 : (W <= 16 ? 16 : 32);
+    static constexpr int GS = NA <= 8 ? 8 : (NA <= 16 ? 16 : 32);
     static constexpr int G = 32 / GS;
     // column stride of the matrix in shared memory, odd: the lanes of a group store and read their
     // columns (and rows) at element strides that fall on distinct banks
     static constexpr int LD = NA | 1;
 };
 
-// Warps per block and the blocks an SM should hold, per instantiation: the tangent kernels with the
-// augmented column apart keep two dense slots per warp next to each thread's dual-number constants in
-// shared memory, which fits three blocks of two warps per SM (four-warp blocks would fit one).
+// Warps per block and the blocks per SM the register allocation aims at, per instantiation (the forward
+// kernels' count measured; a build may set BMC_FWD_MIN_BLOCKS for a sweep).
+#ifndef BMC_FWD_MIN_BLOCKS
+#define BMC_FWD_MIN_BLOCKS 3
+#endif
 template <int NC, int NT>
 struct ChainLaunch {
-    static constexpr int kWarps = (DenseGroup<NC>::kApart && NT > 0) ? 2 : 4;
-    static constexpr int kMinBlocks = NT == 0 ? 3 : (DenseGroup<NC>::kApart ? 3 : 2);
+    static constexpr int kWarps = 4;
+    static constexpr int kMinBlocks = NT == 0 ? BMC_FWD_MIN_BLOCKS : 2;
 };
 
 template <int NC, typename R, int NT>
@@ -111,8 +106,6 @@ struct Dense {
     static constexpr int GS = DenseGroup<NC>::GS;
     static constexpr int G = DenseGroup<NC>::G;
     static constexpr int LD = DenseGroup<NC>::LD;
-    static constexpr bool kApart = DenseGroup<NC>::kApart;
-    static constexpr int W = DenseGroup<NC>::W;
 
     // y = X_A v + C * caug: one column of X times a column of the matrix being built
     static __device__ __forceinline__ void matvec_aug(const SL* sl, const State<NC, D>& v, R caug,
@@ -140,18 +133,11 @@ struct Dense {
     // dt / 2^s): the degree-m Horner recurrence T = I + X T / k, k = m .. 1, then s squarings through the
     // slot's matrix (column j of T T is sum_l T[:, l] T[l][j]). Every lane of the warp calls it (the
     // squarings synchronise the warp, up to the warp's largest count smax); lanes with `work` compute.
-    // With the augmented column apart, lane gl also returns entry gl of that column in `phi` (the
-    // column's state part; its last entry is 1): every lane runs the column's Horner recurrence
-    // phi <- (A phi + C) / k, and each squaring's phi' = E phi + phi is formed row by row, lane gl taking
-    // row gl of E from the shared matrix.
     static __device__ __forceinline__ void exp_column(SL* sl, int gl, bool work, int s, int smax, State<NC, D>& col,
-                                                      D& phi, const TaylorTable& tt) {
-        const R caug = (!kApart && gl == N) ? R(1) : R(0);
+                                                      const TaylorTable& tt) {
+        const R caug = (gl == N) ? R(1) : R(0);
         unit(col, gl);
-        phi = dconst<R, NT>(R(0));
         if (work) {
-            State<NC, D> ph;
-            if constexpr (kApart) unit(ph, -1);
             for (int k = tt.dense_m; k >= 1; --k) {
                 State<NC, D> y;
                 matvec_aug(sl, col, caug, y);
@@ -160,22 +146,14 @@ struct Dense {
                 unit(e, gl);
                 C::axpy_state(e, y);
                 col = e;
-                if constexpr (kApart) {
-                    State<NC, D> yp;
-                    matvec_aug(sl, ph, R(1), yp);
-                    C::scal_state(yp, R(tt.inv_k[k]));
-                    ph = yp;
-                }
             }
-            if constexpr (kApart) phi = C::at(ph, gl);
         }
         for (int q = 0; q < smax; ++q) {
             const bool sq = work && q < s;
             if (sq) {
 #pragma unroll
                 for (int i = 0; i < N; ++i) sl->mat[gl * LD + i] = C::at(col, i);
-                if constexpr (kApart) sl->mat[N * LD + gl] = phi;
-                else sl->mat[gl * LD + N] = dconst<R, NT>(caug);
+                sl->mat[gl * LD + N] = dconst<R, NT>(caug);
             }
             __syncwarp();
             if (sq) {
@@ -187,12 +165,7 @@ struct Dense {
 #pragma unroll
                     for (int i = 0; i < N; ++i) C::at(nc, i) = dfma(sl->mat[l * LD + i], w, C::at(nc, i));
                 }
-                if constexpr (kApart) {       // phi'[gl] = sum_l E[gl][l] phi[l] + phi[gl]
-                    D acc = sl->mat[N * LD + gl];
-#pragma unroll
-                    for (int l = 0; l < N; ++l) acc = dfma(sl->mat[l * LD + gl], sl->mat[N * LD + l], acc);
-                    phi = acc;
-                } else if (caug != R(0)) {    // the augmented column also picks up T[:, aug]
+                if (caug != R(0)) {           // the augmented column also picks up T[:, aug]
 #pragma unroll
                     for (int i = 0; i < N; ++i) C::at(nc, i) = C::at(nc, i) + sl->mat[N * LD + i];
                 }
@@ -249,17 +222,15 @@ struct Dense {
             }
             __syncwarp();
             SL* sl = &sm->slot[grp];
-            const bool work = grp_owner >= 0 && gl < W;
+            const bool work = grp_owner >= 0 && gl < NA;
             const int s = grp_owner >= 0 ? sl->s : 0;
             const int smax = (int)__reduce_max_sync(kFull, (unsigned)s);
             State<NC, D> col;
-            D phi;
-            exp_column(sl, gl, work, s, smax, col, phi, tt);
+            exp_column(sl, gl, work, s, smax, col, tt);
             // M <- T [M; 1]
             if (work) {
 #pragma unroll
                 for (int i = 0; i < N; ++i) sl->mat[gl * LD + i] = C::at(col, i);
-                if constexpr (kApart) sl->mat[N * LD + gl] = phi;
             }
             __syncwarp();
             if (grp_owner >= 0 && gl < N) {
@@ -307,12 +278,10 @@ struct Dense {
             const int Lw = (int)__reduce_max_sync(kFull, (unsigned)(my_slot >= 0 ? L : 0));
             const int rw = (int)__reduce_max_sync(kFull, (unsigned)(my_slot >= 0 ? r : 0));
             SL* sl = &sm->slot[grp];
-            const bool work = grp_owner >= 0 && gl < W;
-            const R pa = (!kApart && gl == N) ? R(1) : R(0); // P's augmented row entry in this column
+            const bool work = grp_owner >= 0 && gl < NA;
+            const R pa = (gl == N) ? R(1) : R(0);          // P's augmented row entry in this column
             State<NC, D> P;
             unit(P, gl);
-            State<NC, D> p;                                 // with kApart: P's augmented column, every lane
-            unit(p, -1);
             for (int k = 0; k < Lw; ++k) {
                 if (my_slot >= 0) {                          // the owner prepares its event k
                     SL* so = &sm->slot[my_slot];
@@ -379,28 +348,12 @@ struct Dense {
                     const int s = dense ? sl->s : 0;
                     const int smax = (int)__reduce_max_sync(kFull, (unsigned)s);
                     State<NC, D> T;
-                    D phiT;
-                    exp_column(sl, gl, dense, s, smax, T, phiT, tt);
+                    exp_column(sl, gl, dense, s, smax, T, tt);
                     if (dense) {
 #pragma unroll
                         for (int i = 0; i < N; ++i) sl->mat[gl * LD + i] = C::at(T, i);
-                        if constexpr (kApart) sl->mat[N * LD + gl] = phiT;
                     }
                     __syncwarp();
-                    if constexpr (kApart) {                  // p <- E p + phi, row gl by lane gl, then shared
-                        D pn = dconst<R, NT>(R(0));
-                        if (dense) {
-                            pn = sl->mat[N * LD + gl];
-#pragma unroll
-                            for (int l = 0; l < N; ++l) pn = dfma(sl->mat[l * LD + gl], C::at(p, l), pn);
-                            sl->vec[gl] = pn;
-                        }
-                        __syncwarp();
-                        if (dense) {
-#pragma unroll
-                            for (int i = 0; i < N; ++i) C::at(p, i) = sl->vec[i];
-                        }
-                    }
                     if (dense) {                             // column gl of T [P; pa]
                         State<NC, D> np;
                         unit(np, -1);
@@ -430,31 +383,15 @@ struct Dense {
                             ca = R(0);
                             C::axpy_state(P, term);
                         }
-                        if constexpr (kApart) {              // ... and the augmented column, [p; 1]
-                            State<NC, D> tp = p;
-                            R cp = R(1);
-                            for (int q = 1; q <= m; ++q) {
-                                State<NC, D> y;
-                                matvec_aug(sl, tp, cp, y);
-                                C::scal_state(y, R(tt.inv_k[q]));
-                                tp = y;
-                                cp = R(0);
-                                C::axpy_state(p, tp);
-                            }
-                        }
                     }
                 }
-                if (work && (kd & 4)) {
-                    C::spoil(P);
-                    if constexpr (kApart) C::spoil(p);
-                }
+                if (work && (kd & 4)) C::spoil(P);
                 __syncwarp();
             }
             // M <- P^r [M; 1]
             if (work) {
 #pragma unroll
                 for (int i = 0; i < N; ++i) sl->mat[gl * LD + i] = C::at(P, i);
-                if constexpr (kApart) sl->mat[N * LD + gl] = C::at(p, gl);
             }
             if (my_slot >= 0) {
                 SL* so = &sm->slot[my_slot];

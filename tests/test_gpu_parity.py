@@ -220,8 +220,8 @@ def test_repeated_block_pulses_match_the_oracle(cuda, nc, n_pulses):
 
 @pytest.mark.parametrize("nc", [4, 5])
 def test_dense_path_tangents_with_many_pools(cuda, nc):
-    """2 s CW blocks (every event on the dense path) with four and five CEST pools plus MT: with four, the
-    augmented column is kept apart and two chains share a warp; Z and tangents against the oracle."""
+    """2 s CW blocks (every event on the dense path, a whole warp per chain) with four and five CEST pools
+    plus MT: Z and tangents against the oracle."""
     from bmc_b200.design import jacobian
     from bmc_b200.fitting import Experiment, FitSpec, FreeParam
     pb = _random_batch(1, nc, seed=40 + nc, mt=True)
