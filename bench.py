@@ -347,9 +347,10 @@ def run_ours(args, rank, world, local_rank):
                    "taylor_tail": {_lib.F64: "Taylor terms below 1e-6 of the state (bound theta^k/k!) formed in "
                                              "float32, summed into the float64 state once per sub-step; "
                                              "truncation 1e-13 per sub-step",
-                                   _lib.MIXED: "Taylor terms below the state (bound theta^k/k!) formed in float32, "
-                                               "summed into the float64 state once per sub-step; leading terms in "
-                                               "float64; truncation 1e-9 per sub-step",
+                                   _lib.MIXED: "the first Taylor term of every sub-step in float64 (more where their "
+                                               "bound theta^k/k! exceeds 3x the state), later terms in float32, "
+                                               "summed into the float64 state once per sub-step; truncation 1e-9 "
+                                               "per sub-step",
                                    _lib.F32: "all Taylor terms and the state in float32; truncation 2^-24"}[prec]},
         "e2e": {"value": world * nv / (e2e_ms * 1e-3), "unit": "Z-spectra/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms, "steps": e2e_steps},

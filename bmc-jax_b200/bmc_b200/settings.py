@@ -1,8 +1,8 @@
 """Global precision switch, mirroring BMC-JAX `bmc_jax.settings` (settings.py:41-75).
 
 `use_x64(True)` (the default here) runs forward simulations in float64; `use_x64(False)` selects the
-float32 kernel. `use_precision("mixed")` selects the mixed kernel: float64 state and leading Taylor terms,
-float32 for the terms below the state (BMC_MIXED in include/bmc_b200.h). Tangents, Jacobians and
+float32 kernel. `use_precision("mixed")` selects the mixed kernel: float64 state and first Taylor term of every
+sub-step, float32 for the later terms (BMC_MIXED in include/bmc_b200.h). Tangents, Jacobians and
 fits always run in float64. `use_expm` is accepted for compatibility: both of the reference's backends
 ("library", "plain") compute the same matrix exponential, and this library has one kernel for it. No
 environment variable is read.

@@ -106,7 +106,7 @@ TaylorTable make_table(double tol, int m_max, double dense_theta, double dense_s
 #define BMC_MIXED_TOL 1e-9
 #endif
 #ifndef BMC_MIXED_F32
-#define BMC_MIXED_F32 1.0
+#define BMC_MIXED_F32 3.0
 #endif
 
 __device__ TaylorTable g_tables[3];   // [BMC_F64, BMC_F32, BMC_MIXED], per device

@@ -55,11 +55,11 @@ typedef enum {
  * added to the float64 state once per sub-step, at most ~2e-13 of the state per event. Tangents, the
  * dense path for long events and the LM arithmetic are float64 throughout. BMC_F32: float32 Taylor
  * propagation, float64 dense path (about 1e-4 in Z over thousands of pulse samples, the level of the
- * reference's own float32 path). BMC_MIXED: the state and the leading Taylor terms of every sub-step in
- * float64, every term below the state itself (by the series bound) formed in float32, and a truncation
- * tolerance of 1e-9 per sub-step: the float32 rounding enters only through terms smaller than the
- * state, and the state itself is never rounded to float32 (measured: ~4e-10 in Z over the 4,023-event
- * benchmark train). Forward model only; float64 dense path. */
+ * reference's own float32 path). BMC_MIXED: the state and the first Taylor term of every sub-step in
+ * float64 (more leading terms where their bound exceeds three times the state), every later term formed
+ * in float32, and a truncation tolerance of 1e-9 per sub-step: the state itself is never rounded to
+ * float32 (measured: ~4e-10 in Z over the 4,023-event benchmark train). Forward model only; float64
+ * dense path. */
 #define BMC_F64 0
 #define BMC_F32 1
 #define BMC_MIXED 2
