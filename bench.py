@@ -886,14 +886,18 @@ def run_uneven(args, rank, world, local_rank):
 
 
 def lm_tangent_roofline(exp, spec, X_phys, peak):
-    """The LM's tangent pass as the fit runs it (every free parameter's derivative at every offset, one
-    launch per tangent, the primal carried along as dual numbers) on `X_phys`, timed with CUDA events on
-    the launching stream, against the kernel's own counts of the work it executed. Dual-number FLOPs:
-    each primal multiply-add becomes 1 + 2 T (T tangents per launch), so a launch's FLOPs are its counted
-    primal FLOPs times (1 + 2 T)."""
+    """The LM's tangent pass as the fit runs it (every free parameter's derivative at every offset) on
+    `X_phys`, timed with CUDA events on the launching stream, against the kernels' own counts of the work
+    they executed, in both tangent modes. The automatic mode (what bmc_lm_fit runs) takes the adjoint
+    kernel on a single-event table such as the CW ladder: one launch, the exponential and its Frechet
+    derivative in the readout's direction as a pair (dual) -- FLOPs per squaring 6 N^2 (N + 1), per Horner
+    column product two operator products and a rank-one update -- then every tangent by a contraction
+    (not counted: one sparse row per lane and tangent). Forward mode carries each tangent through a launch
+    of its own as dual numbers: each primal multiply-add becomes 1 + 2 T (T tangents per launch), so a
+    launch's FLOPs are its counted primal FLOPs times (1 + 2 T)."""
     import ctypes as C
     import torch
-    from bmc_b200 import _lib
+    from bmc_b200 import _lib, settings
     from bmc_b200.fitting import write_params, field_row
     from bmc_b200.simulation import DeviceEvents, pack_params, problem, tile_params, n_cest_of, state_size
     n = X_phys.shape[0]
@@ -918,28 +922,46 @@ def lm_tangent_roofline(exp, spec, X_phys, peak):
     sh = C.c_void_p(stream.cuda_stream)
     call = lambda: _lib.check(L.bmc_simulate_jvp(pr, _lib.ptr(dP), dev_ev.struct, _lib.ptr(dM), None, tg,
                                                  _lib.ptr(z), _lib.ptr(jz), sh))
-    call()
-    work = torch.zeros(5, dtype=torch.int64, device="cuda")
-    _lib.check(L.bmc_simulate_jvp_counted(pr, _lib.ptr(dP), dev_ev.struct, _lib.ptr(dM), None, tg, _lib.ptr(z),
-                                          _lib.ptr(jz), _lib.ptr(work), sh))
-    torch.cuda.synchronize()
-    terms, hcols, squar, executed, _ = [int(x) for x in work.cpu()]
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    call()
-    e1.record(stream)
-    e1.synchronize()
-    ms = e0.elapsed_time(e1)
-    T = 2 if nc <= 1 else 1                                  # tangents per launch (the library's choice)
     nnz = 12 + 15 * nc
     flop_term = 2 * nnz + 2 * N
-    flops = (terms * flop_term + hcols * flop_term + squar * 2.0 * N * N * (N + 1)) * (1 + 2 * T)
+    T = 2 if nc <= 1 else 1                                  # forward mode's tangents per launch
+    launches_fwd = (P + T - 1) // T
+    out = {}
+    for mode in ("auto", "forward"):
+        settings.use_tangents(mode)
+        try:
+            call()
+            work = torch.zeros(5, dtype=torch.int64, device="cuda")
+            _lib.check(L.bmc_simulate_jvp_counted(pr, _lib.ptr(dP), dev_ev.struct, _lib.ptr(dM), None, tg,
+                                                  _lib.ptr(z), _lib.ptr(jz), _lib.ptr(work), sh))
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            call()
+            e1.record(stream)
+            e1.synchronize()
+            out[mode] = ([int(x) for x in work.cpu()], e0.elapsed_time(e1))
+        finally:
+            settings.use_tangents("auto")
+    (terms, hcols, squar, _, _), ms = out["auto"]
+    (terms_f, hcols_f, squar_f, _, _), ms_f = out["forward"]
+    flops_f = (terms_f * flop_term + hcols_f * flop_term + squar_f * 2.0 * N * N * (N + 1)) * (1 + 2 * T)
+    adjoint = P > 1 and terms == 0 and squar_f == launches_fwd * squar
+    if adjoint:
+        flops = hcols * (2.0 * flop_term + 2 * N) + squar * 6.0 * N * N * (N + 1)
+        kernel = f"adjoint_kernel<{nc}> (LM tangent pass: {P} tangents in 1 launch)"
+    else:
+        flops = flops_f
+        kernel = f"chain_kernel<{nc}, double, {T}> (LM tangent pass, {launches_fwd} launches)"
     tf = flops / (ms * 1e-3) / 1e12
+    tf_f = flops_f / (ms_f * 1e-3) / 1e12
     return {"bound": "fp64-fma", "achieved": tf, "peak": peak, "unit": "TFLOP/s",
-            "frac": tf / peak if peak else None, "traffic": None,
-            "kernel": f"chain_kernel<{nc}, double, {T}> (LM tangent pass, {P} launches)",
+            "frac": tf / peak if peak else None, "traffic": None, "kernel": kernel,
             "voxels": n, "offsets": dev_ev.n_offsets, "ms": ms, "flops": flops, "taylor_terms": terms,
             "dense_columns": hcols, "dense_squarings": squar,
+            "forward_mode": {"ms": ms_f, "launches": launches_fwd, "flops": flops_f, "achieved": tf_f,
+                             "frac": tf_f / peak if peak else None,
+                             "kernel": f"chain_kernel<{nc}, double, {T}>"},
             "peak_source": "the forward leg's FP64 FMA probe of this run (burst)"}
 
 

@@ -21,12 +21,14 @@ MAX_TANGENTS = 8
 F64, F32, MIXED = 0, 1, 2
 SEED_NONE, SEED_SPREAD_SIGMA = -1, -2
 SLOT_SPREAD_SIGMA, SLOT_M_START = -2, -3
+TANGENTS_AUTO, TANGENTS_FORWARD = 0, 1
 
 EXPORTS = ("bmc_abi_version", "bmc_version", "bmc_last_error", "bmc_release", "bmc_simulate",
            "bmc_simulate_jvp", "bmc_simulate_trajectory", "bmc_lm_fit", "bmc_normal_blocks",
            "bmc_simulate_counted", "bmc_simulate_jvp_counted", "bmc_probe_fma_peak", "bmc_simulate_noalloc",
            "bmc_mlp_sizes", "bmc_mlp_sync", "bmc_mlp_forward", "bmc_mlp_backward", "bmc_mlp_adam_step", "bmc_uneven_create", "bmc_uneven_simulate",
-           "bmc_uneven_destroy", "bmc_uneven_set_dense_switch", "bmc_normal_segments", "bmc_schur_step", "bmc_schur_eliminate", "bmc_schur_back")
+           "bmc_uneven_destroy", "bmc_uneven_set_dense_switch", "bmc_normal_segments", "bmc_schur_step", "bmc_schur_eliminate", "bmc_schur_back",
+           "bmc_set_tangent_mode")
 
 
 class Problem(C.Structure):
@@ -104,6 +106,8 @@ def lib():
         L.bmc_simulate_jvp_counted.restype = C.c_int
         L.bmc_probe_fma_peak.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double), vp]
         L.bmc_probe_fma_peak.restype = C.c_int
+        L.bmc_set_tangent_mode.argtypes = [C.c_int32]
+        L.bmc_set_tangent_mode.restype = C.c_int
         L.bmc_simulate_noalloc.argtypes = [C.POINTER(Problem), vp, C.POINTER(Events), vp, C.POINTER(Spread), vp, vp]
         L.bmc_simulate_noalloc.restype = C.c_int
         i32p = C.POINTER(C.c_int32)

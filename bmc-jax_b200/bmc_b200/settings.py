@@ -4,12 +4,16 @@
 float32 kernel. `use_precision("mixed")` selects the mixed kernel: float64 state and first Taylor term of every
 sub-step, float32 for the later terms (BMC_MIXED in include/bmc_b200.h). Tangents, Jacobians and
 fits always run in float64. `use_expm` is accepted for compatibility: both of the reference's backends
-("library", "plain") compute the same matrix exponential, and this library has one kernel for it. No
-environment variable is read.
+("library", "plain") compute the same matrix exponential, and this library has one kernel for it.
+`use_tangents("forward")` keeps Jacobians in forward mode (one dual-number launch per tangent) where
+"auto" (the default) computes every tangent of a single-event table -- CW Z-spectra, B1 ladders -- from
+one Frechet derivative of the exponential (bmc_set_tangent_mode in include/bmc_b200.h); both give the same
+derivatives to rounding. No environment variable is read.
 """
-_STATE = {"precision": "f64", "expm": "library"}
+_STATE = {"precision": "f64", "expm": "library", "tangents": "auto"}
 EXPM_BACKENDS = ("library", "plain")
 PRECISIONS = ("f64", "mixed", "f32")
+TANGENT_MODES = ("auto", "forward")
 
 
 def use_x64(enable: bool = True) -> bool:
@@ -44,3 +48,17 @@ def use_expm(backend: str = "library") -> str:
 
 def expm_backend() -> str:
     return _STATE["expm"]
+
+
+def use_tangents(mode: str = "auto") -> str:
+    """Select how Jacobians are computed: "auto" or "forward" (process-wide, in the library)."""
+    if mode not in TANGENT_MODES:
+        raise ValueError(f"use_tangents: one of {TANGENT_MODES}, not {mode!r}")
+    from . import _lib
+    _lib.check(_lib.lib().bmc_set_tangent_mode(_lib.TANGENTS_AUTO if mode == "auto" else _lib.TANGENTS_FORWARD))
+    _STATE["tangents"] = mode
+    return mode
+
+
+def tangent_mode() -> str:
+    return _STATE["tangents"]

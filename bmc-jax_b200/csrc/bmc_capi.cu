@@ -22,6 +22,7 @@
 
 #include "bmc_lm.cuh"
 #include "bmc_joint.cuh"
+#include "bmc_adjoint.cuh"
 
 using namespace bmc;
 
@@ -297,6 +298,51 @@ bmc_status launch_chain(const ChainArgs& a, const TaylorTable* tt, cudaStream_t 
     return BMC_OK;
 }
 
+// Tangent mode (bmc_set_tangent_mode): BMC_TANGENTS_AUTO takes the adjoint kernel where it applies.
+std::atomic<int> g_tangent_mode{BMC_TANGENTS_AUTO};
+
+template <int NC>
+bmc_status launch_adjoint(const ChainArgs& a, const int* row_ev, int n_tan, const TaylorTable* tt, cudaStream_t st) {
+    const size_t smem = kAdjWarps * DenseGroup<NC>::G * sizeof(AdjSlot<NC>);
+    static std::atomic<unsigned long long> configured{0};
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev >= 64 || !((configured.load(std::memory_order_acquire) >> dev) & 1ull)) {
+        CUDA_TRY(cudaFuncSetAttribute(adjoint_kernel<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        if (dev < 64) configured.fetch_or(1ull << dev, std::memory_order_acq_rel);
+    }
+    const long long nch = (long long)a.n_vox * a.n_off;
+    const long long blocks = (nch + kAdjWarps * 32 - 1) / (kAdjWarps * 32);
+    if (blocks > 0x7fffffffLL) return fail(BMC_ERR_INVALID, "%lld chains exceed one launch", nch);
+    if (blocks == 0) return BMC_OK;
+    adjoint_kernel<NC><<<(unsigned)blocks, kAdjWarps * 32, smem, st>>>(a, row_ev, n_tan, tt);
+    CUDA_TRY(cudaGetLastError());
+    return BMC_OK;
+}
+
+// Whether the tangents of a uniform table go through the adjoint kernel: two or more tangents, the
+// automatic mode, and every row a single-event row (adjoint_rows_kernel, which also fills row_ev). The
+// check reads one flag back, so a stream being captured keeps forward mode.
+bmc_status use_adjoint(const EvRec<double>* rec, const bmc_problem* pr, int n_tan, int* row_ev, int* flag,
+                       cudaStream_t st, bool* ok) {
+    *ok = false;
+    if (n_tan < 2 || g_tangent_mode.load(std::memory_order_relaxed) != BMC_TANGENTS_AUTO || pr->mz_loc < 0 ||
+        pr->n_events < 1 || pr->n_offsets < 1)
+        return BMC_OK;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CUDA_TRY(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return BMC_OK;
+    CUDA_TRY(cudaMemsetAsync(flag, 1, sizeof(int), st));    // nonzero: every row so far qualifies
+    adjoint_rows_kernel<<<(pr->n_offsets + 127) / 128, 128, 0, st>>>(rec, pr->n_offsets, pr->n_events,
+                                                                      pr->reset_after_adc, row_ev, flag);
+    CUDA_TRY(cudaGetLastError());
+    int h = 0;
+    CUDA_TRY(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    *ok = h != 0;
+    return BMC_OK;
+}
+
 // Order the chains by estimated cost: `order` and the sort's scratch are carved from `cv`.
 template <int NC, typename R>
 bmc_status order_chains(ChainArgs& a, Carve& cv, cudaStream_t st) {
@@ -474,7 +520,7 @@ struct Impl {
         void* ws = nullptr;
         const long long nch = (long long)pr->n_voxels * pr->n_offsets;
         if ((s = workspace(align256(nrec * sizeof(EvRec<double>)) + 256 + align256(sizeof(int4) * pr->n_offsets) +
-                               order_bytes(nch), st, &ws)) != BMC_OK)
+                               align256(sizeof(int) * pr->n_offsets) + 256 + order_bytes(nch), st, &ws)) != BMC_OK)
             return s;
         Carve cv(ws);
         ChainArgs a{};
@@ -492,7 +538,12 @@ struct Impl {
         a.seg = cv.take<int4>(pr->n_offsets);
         if ((s = scan_blocks(rec, pr->n_offsets, pr->n_events, pr->n_offsets, const_cast<int4*>(a.seg), st)) != BMC_OK)
             return s;
+        int* row_ev = cv.take<int>(pr->n_offsets);
+        int* flag = cv.take<int>(1);
+        bool adj = false;
+        if ((s = use_adjoint(rec, pr, tg->n_tangents, row_ev, flag, st, &adj)) != BMC_OK) return s;
         if ((s = order_chains<NC, double>(a, cv, st)) != BMC_OK) return s;
+        if (adj) return launch_adjoint<NC>(a, row_ev, tg->n_tangents, tt, st);
         return run_tangents<NC>(a, tg->n_tangents, tt, st);
     }
 
@@ -511,7 +562,7 @@ struct Impl {
                              2 * align256(sizeof(double) * nv * no) + align256(sizeof(double) * P * nv * no) +
                              2 * align256(sizeof(double) * nv * P) + 2 * align256(sizeof(double) * nv) +
                              align256(sizeof(int) * nv) + align256(sizeof(int4) * no) + 4096 +
-                             order_bytes((long long)nv * no);
+                             align256(sizeof(int) * no) + 256 + order_bytes((long long)nv * no);
         void* ws = nullptr;
         if ((s = workspace(bytes, st, &ws)) != BMC_OK) return s;
         Carve cv(ws);
@@ -534,6 +585,8 @@ struct Impl {
         int* need = cv.take<int>(nv);
         int4* seg = cv.take<int4>(no);
         int* status = cv.take<int>(1);
+        int* row_ev = cv.take<int>(no);
+        int* flag = cv.take<int>(1);
         if ((s = prep_events<double>(pr, ev, rec, st)) != BMC_OK) return s;
         CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), st));
         CUDA_TRY(cudaMemcpyAsync(x, x0, sizeof(double) * nv * P, cudaMemcpyDeviceToDevice, st));
@@ -557,6 +610,8 @@ struct Impl {
         const double* sig0 = sp ? sp->d_sigma_hz : nullptr;
         a.ev = rec; a.status = status; a.seg = seg;
         if ((s = scan_blocks(rec, no, pr->n_events, no, seg, st)) != BMC_OK) return s;
+        bool adj = false;
+        if ((s = use_adjoint(rec, pr, P, row_ev, flag, st, &adj)) != BMC_OK) return s;
         a.params = params; a.m0 = m0;
         if ((s = order_chains<NC, double>(a, cv, st)) != BMC_OK) return s;
         for (int p = 0; p < P; ++p) a.field_row[p] = fs->field_row[p] == BMC_SLOT_M_START ? BMC_SEED_NONE : fs->field_row[p];
@@ -569,7 +624,8 @@ struct Impl {
             ChainArgs aj = a;
             aj.params = px; aj.m0 = m0x; aj.sigma = sp ? sgx : nullptr; aj.seed = seed; aj.dm0 = has_m ? dm0 : nullptr;
             aj.active = need; aj.out = z; aj.jout = J;
-            if ((s = run_tangents<NC>(aj, P, tt, st)) != BMC_OK) return s;
+            if ((s = adj ? launch_adjoint<NC>(aj, row_ev, P, tt, st) : run_tangents<NC>(aj, P, tt, st)) != BMC_OK)
+                return s;
             lm_solve_kernel<<<wb, 128, 0, st>>>(nv, no, fs->n_points_skip, ss, z, zm, J, fs->d_free, x, lam, cost, xt);
             CUDA_TRY(cudaGetLastError());
             // the trial point
@@ -686,6 +742,13 @@ bmc_status check_jvp(const bmc_problem* prob, const double* d_params, const bmc_
     return BMC_OK;
 }
 }  // namespace
+
+bmc_status bmc_set_tangent_mode(int32_t mode) {
+    if (mode != BMC_TANGENTS_AUTO && mode != BMC_TANGENTS_FORWARD)
+        return fail(BMC_ERR_INVALID, "tangent mode %d: BMC_TANGENTS_AUTO or BMC_TANGENTS_FORWARD", mode);
+    g_tangent_mode.store(mode, std::memory_order_relaxed);
+    return BMC_OK;
+}
 
 bmc_status bmc_simulate_jvp_counted(const bmc_problem* prob, const double* d_params, const bmc_events* ev,
                                     const double* d_m0, const bmc_spread* spread, const bmc_tangents* tan,

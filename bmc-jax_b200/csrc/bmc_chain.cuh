@@ -98,20 +98,26 @@ struct Chain {
     // ---------------------------------------------------------------------------------------------
     // parameters -> per-chain constants (matrix.py:99-173), with tangents seeded per field row
     // ---------------------------------------------------------------------------------------------
-    static __device__ __forceinline__ D field(const ChainArgs& a, int row, int v) {
+    // tangents t0 .. t0 + NT - 1 of the launch's set (a.t0 in the chain kernel; the adjoint kernel seeds
+    // one tangent per lane)
+    static __device__ __forceinline__ D field(const ChainArgs& a, int row, int v, int t0) {
         D r = dconst<R, NT>(R(a.params[(size_t)row * a.n_vox + v]));
         if constexpr (NT > 0) {
 #pragma unroll
             for (int t = 0; t < NT; ++t)
-                if (a.field_row[a.t0 + t] == row) r.d[t] = R(a.seed[(size_t)(a.t0 + t) * a.n_vox + v]);
+                if (a.field_row[t0 + t] == row) r.d[t] = R(a.seed[(size_t)(t0 + t) * a.n_vox + v]);
         }
         return r;
     }
 
     static __device__ void load_const(const ChainArgs& a, int v, int node, ChainConst<NC, D>& cc) {
-        const D r1w = field(a, L::WR1, v), r2w = field(a, L::WR2, v);
-        const D b0 = field(a, L::B0, v), gam = field(a, L::GAM, v);
-        D b0i = field(a, L::B0I, v);
+        load_const(a, v, node, cc, a.t0);
+    }
+
+    static __device__ void load_const(const ChainArgs& a, int v, int node, ChainConst<NC, D>& cc, int t0) {
+        const D r1w = field(a, L::WR1, v, t0), r2w = field(a, L::WR2, v, t0);
+        const D b0 = field(a, L::B0, v, t0), gam = field(a, L::GAM, v, t0);
+        D b0i = field(a, L::B0I, v, t0);
         const D larmor = R(1e6) * (gam * b0);
         if (a.n_nodes > 1 || a.sigma) {
             // isochromat `node`: b0_inhom + sigma u / (gamma b0 / 2 pi)   (spread.py:101-104)
@@ -119,7 +125,7 @@ struct Chain {
             if constexpr (NT > 0) {
 #pragma unroll
                 for (int t = 0; t < NT; ++t)
-                    if (a.field_row[a.t0 + t] == -2) sig.d[t] = R(a.seed[(size_t)(a.t0 + t) * a.n_vox + v]);
+                    if (a.field_row[t0 + t] == -2) sig.d[t] = R(a.seed[(size_t)(t0 + t) * a.n_vox + v]);
             }
             const D hzpp = R(1.0 / 6.283185307179586) * (gam * b0);
             b0i = b0i + (R(a.u[node]) * sig) / hzpp;
@@ -128,9 +134,9 @@ struct Chain {
         D ksum = dconst<R, NT>(R(0));
 #pragma unroll
         for (int i = 0; i < NC; ++i) {
-            const D k = field(a, L::CK + i, v), f = field(a, L::CF + i, v);
-            const D r1 = field(a, L::CR1 + i, v), r2 = field(a, L::CR2 + i, v);
-            const D dw = field(a, L::CDW + i, v);
+            const D k = field(a, L::CK + i, v, t0), f = field(a, L::CF + i, v, t0);
+            const D r1 = field(a, L::CR1 + i, v, t0), r2 = field(a, L::CR2 + i, v, t0);
+            const D dw = field(a, L::CDW + i, v, t0);
             cc.k[i] = k;
             cc.kwc[i] = k * f;
             ksum = ksum + cc.kwc[i];
@@ -139,8 +145,8 @@ struct Chain {
             cc.cc[i] = r1 * f;
             cc.offc0[i] = R(1e-6) * (dw * larmor);
         }
-        const D kmt = field(a, L::MK, v), fmt = field(a, L::MF, v), r1mt = field(a, L::MR1, v);
-        const D r2mt = field(a, L::MR2, v), dwmt = field(a, L::MDW, v);
+        const D kmt = field(a, L::MK, v, t0), fmt = field(a, L::MF, v, t0), r1mt = field(a, L::MR1, v, t0);
+        const D r2mt = field(a, L::MR2, v, t0), dwmt = field(a, L::MDW, v, t0);
         cc.kmt = kmt;
         cc.kwmt = kmt * fmt;
         cc.Rm1 = r1mt + kmt;
@@ -148,7 +154,7 @@ struct Chain {
         cc.Rw2 = r2w + ksum;
         cc.Rw1 = (r1w + ksum) + cc.kwmt;
         cc.cw = r1w;
-        cc.relb1 = field(a, L::RB1, v);
+        cc.relb1 = field(a, L::RB1, v, t0);
         cc.dwmt = R(1e-6) * (dwmt * larmor);
         cc.t2mt = dconst<R, NT>(R(1)) / r2mt;
         cc.w0sl = R(1e-6) * larmor;
@@ -299,80 +305,6 @@ struct Chain {
         y.zm = zm;
     }
 
-    // The first term of a sub-step, y = X [v; 1] with X = [A C; 0 0] h, its scaled coefficients formed from
-    // the chain constants where each row needs them: the arithmetic of event_coef, scale_coef and
-    // matvec<true> exactly, without the full set of float64 coefficients held next to the state and the
-    // term (the mixed kernel's register peak). Float64 kernel without tangents only.
-    static __device__ __forceinline__ void first_term(const ChainConst<NC, D>& cc, const EvRec<R>& e, D g_mt, R h,
-                                                      const State<NC, D>& v, State<NC, D>& y) {
-        static_assert(NT == 0, "the streamed first term carries no tangents");
-        const R offw_u = e.wf - cc.dw0.v;
-        const R w1 = e.w1 * cc.relb1.v;
-        const R offw = h * offw_u, w1x = h * (e.c * w1), w1y = h * (e.s * w1);
-        const R Rw2 = h * cc.Rw2.v, Rw1 = h * cc.Rw1.v;
-        R xw = fma(offw, v.yw.v, -(Rw2 * v.xw.v));
-        xw = xw - w1y * v.zw.v;
-        R yw = fma(w1x, v.zw.v, -(Rw2 * v.yw.v));
-        yw = yw - offw * v.xw.v;
-        R zw = fma(w1y, v.xw.v, -(Rw1 * v.zw.v));
-        zw = zw - w1x * v.yw.v;
-        R zm = fma(h * cc.kwmt.v, v.zw.v, -((h * (cc.Rm1.v + (w1 * w1) * g_mt.v)) * v.zm.v));
-        zw = fma(cc.cw.v, h, zw);
-        zm = fma(cc.cm.v, h, zm);
-        R px = R(0), py = R(0), pz = (h * cc.kmt.v) * v.zm.v;
-#pragma unroll
-        for (int i = 0; i < NC; ++i) {
-            const R k = h * cc.k[i].v, kwc = h * cc.kwc[i].v, Rc2 = h * cc.Rc2[i].v, Rc1 = h * cc.Rc1[i].v;
-            const R offc = h * (cc.offc0[i].v - offw_u);
-            px = fma(k, v.xc[i].v, px);
-            py = fma(k, v.yc[i].v, py);
-            pz = fma(k, v.zc[i].v, pz);
-            R xc = fma(kwc, v.xw.v, -(Rc2 * v.xc[i].v));
-            xc = xc - offc * v.yc[i].v;
-            xc = xc - w1y * v.zc[i].v;
-            R yc = fma(kwc, v.yw.v, -(Rc2 * v.yc[i].v));
-            yc = fma(offc, v.xc[i].v, yc);
-            yc = fma(w1x, v.zc[i].v, yc);
-            R zc = fma(kwc, v.zw.v, -(Rc1 * v.zc[i].v));
-            zc = fma(w1y, v.xc[i].v, zc);
-            zc = zc - w1x * v.yc[i].v;
-            zc = fma(cc.cc[i].v, h, zc);
-            y.xc[i].v = xc;
-            y.yc[i].v = yc;
-            y.zc[i].v = zc;
-        }
-        y.xw.v = xw + px;
-        y.yw.v = yw + py;
-        y.zw.v = zw + pz;
-        y.zm.v = zm;
-    }
-
-    // The sub-step's scaled coefficients in float32, each formed in float64 as event_coef and scale_coef
-    // form it and rounded once (what converting the float64 set gives), one at a time.
-    template <typename S32>
-    static __device__ __forceinline__ void coef32(const ChainConst<NC, D>& cc, const EvRec<R>& e, D g_mt, R h,
-                                                  S32& s) {
-        static_assert(NT == 0, "float32 coefficients carry no tangents");
-        const R offw_u = e.wf - cc.dw0.v;
-        const R w1 = e.w1 * cc.relb1.v;
-        s.offw.v = float(h * offw_u);
-        s.w1x.v = float(h * (e.c * w1));
-        s.w1y.v = float(h * (e.s * w1));
-        s.Rw2.v = float(h * cc.Rw2.v);
-        s.Rw1.v = float(h * cc.Rw1.v);
-#pragma unroll
-        for (int i = 0; i < NC; ++i) {
-            s.k[i].v = float(h * cc.k[i].v);
-            s.kwc[i].v = float(h * cc.kwc[i].v);
-            s.Rc2[i].v = float(h * cc.Rc2[i].v);
-            s.Rc1[i].v = float(h * cc.Rc1[i].v);
-            s.offc[i].v = float(h * (cc.offc0[i].v - offw_u));
-        }
-        s.kmt.v = float(h * cc.kmt.v);
-        s.kwmt.v = float(h * cc.kwmt.v);
-        s.Rm1W.v = float(h * (cc.Rm1.v + (w1 * w1) * g_mt.v));
-    }
-
     static __device__ __forceinline__ void axpy_state(State<NC, D>& acc, const State<NC, D>& t) {
         acc.xw = acc.xw + t.xw; acc.yw = acc.yw + t.yw; acc.zw = acc.zw + t.zw; acc.zm = acc.zm + t.zm;
 #pragma unroll
@@ -434,34 +366,19 @@ struct Chain {
                 pend &= ~__ballot_sync(0xffffffffu, member);
                 ++passes;
                 const int m_on = member ? m_own : 0;
+                StepCoef<NC, D> s;
+                event_coef(cst, rec, g_mt, s);
+                scale_coef(s, h);
                 State<NC, D> term;
+                matvec<true>(s, M, term, &cst, h);
+                fma_state(M, member ? R(1) : R(0), term);
                 int k = 2;
-                // the float64 terms below the switch point, from the full set of scaled coefficients
-                auto float64_terms = [&]() {
-                    StepCoef<NC, D> s;
-                    event_coef(cst, rec, g_mt, s);
-                    scale_coef(s, h);
-                    matvec<true>(s, M, term, &cst, h);
-                    fma_state(M, member ? R(1) : R(0), term);
 #pragma unroll 1
-                    for (; k <= m_w && k < k32; ++k) {
-                        State<NC, D> nt;
-                        matvec<false>(s, term, nt);
-                        term = nt;
-                        fma_state(M, k <= m_on ? R(tt.inv_fact[k]) : R(0), term);
-                    }
-                };
-                if constexpr (kMixed) {
-                    if (k32 <= 2) {
-                        // only the first term in float64 (the mixed table's usual case): streamed from the
-                        // chain constants, so that no float64 coefficient set is held next to the state
-                        first_term(cst, rec, g_mt, h, M, term);
-                        fma_state(M, member ? R(1) : R(0), term);
-                    } else {
-                        float64_terms();
-                    }
-                } else {
-                    float64_terms();
+                for (; k <= m_w && k < k32; ++k) {
+                    State<NC, D> nt;
+                    matvec<false>(s, term, nt);
+                    term = nt;
+                    fma_state(M, k <= m_on ? R(tt.inv_fact[k]) : R(0), term);
                 }
                 if constexpr (kMixed) {
                     if (k <= m_w) {
@@ -469,7 +386,7 @@ struct Chain {
                         using F = Dn<float, 0>;
                         StepCoef<NC, F> s32;
                         State<NC, F> t32, a32;
-                        coef32(cst, rec, g_mt, h, s32);
+                        to_float(s, s32);
                         to_float(term, t32);
                         zero_state(a32);
 #pragma unroll 1

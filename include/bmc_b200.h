@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define BMC_ABI_VERSION 2
+#define BMC_ABI_VERSION 3
 #define BMC_MAX_CEST 5             /* water + up to five CEST pools + MT: N <= 19 */
 #define BMC_MAX_TANGENTS 8
 #define BMC_N_FIELDS(n_cest) (13 + 5 * (n_cest))
@@ -159,7 +159,21 @@ bmc_status bmc_simulate_trajectory(const bmc_problem* prob, const double* d_para
  * Replaces the jax.jacfwd of the model in fitting/lm.py:39, fitting/joint.py:300,317 and
  * design/crlb.py:57. d_z: [n_voxels][n_offsets]; d_jz: [n_tangents][n_voxels][n_offsets]
  * (state index prob->mz_loc, which must be >= 0).
+ *
+ * Two kernels compute the same derivatives. Forward mode carries every tangent through every event as
+ * a dual number (one launch per tangent; two per launch for at most one CEST pool). Where each row's
+ * state evolves in a single event -- an RF block or a delay; no spoiler or gradient; no readout that
+ * resets the state before the row ends: the CW Z-spectra and B1 ladders -- and two or more tangents are
+ * asked for, one launch computes the Frechet derivative of that event's exponential in the readout's
+ * direction, and every tangent follows from it (reverse mode through the exponential). The results agree
+ * to rounding (~1e-12 relative). bmc_lm_fit chooses the same way. Choosing reads one flag back from
+ * the device (a stream synchronisation), so a stream being captured into a CUDA graph keeps forward
+ * mode. bmc_set_tangent_mode(BMC_TANGENTS_FORWARD) makes forward mode the only one (process-wide);
+ * BMC_TANGENTS_AUTO (the default) restores the choice.
  */
+#define BMC_TANGENTS_AUTO 0
+#define BMC_TANGENTS_FORWARD 1
+bmc_status bmc_set_tangent_mode(int32_t mode);
 bmc_status bmc_simulate_jvp(const bmc_problem* prob, const double* d_params, const bmc_events* ev,
                             const double* d_m0, const bmc_spread* spread, const bmc_tangents* tan,
                             double* d_z, double* d_jz, void* stream);
@@ -326,8 +340,10 @@ bmc_status bmc_mlp_adam_step(const bmc_mlp_shape* shape, float* d_params, const 
  *   each), [1] dense-path Horner column products, [2] dense-path squarings, [3] Taylor terms executed
  *   (a warp runs to the largest need among its chains), [4] of the terms in [0], those formed in float32.
  * bmc_simulate_jvp_counted: bmc_simulate_jvp that adds the same five counts to d_work[5], summed over
- *   its launches: one per tangent (two per launch for at most one CEST pool), each carrying the primal
- *   and its tangents through the same steps as dual numbers.
+ *   its launches: in forward mode one per tangent (two per launch for at most one CEST pool), each
+ *   carrying the primal and its tangents through the same steps as dual numbers; in the adjoint kernel
+ *   one launch whose [1] counts the Horner column products of the pair (exp, Frechet derivative) and
+ *   [2] its squarings.
  * bmc_probe_fma_peak: launches `blocks` x 256 threads of 8 independent FMA chains x `iters`
  *   (float64 or float32) and returns the FLOPs one launch executes, to time against.
  */

@@ -72,3 +72,16 @@ def test_fit_spec_is_validated():
     spec.field_row[0] = _lib.SLOT_SPREAD_SIGMA
     with pytest.raises(RuntimeError, match="needs a spread"):
         _lib.check(L.bmc_lm_fit(pr, dummy, ev, dummy, None, spec, dummy, dummy, dummy, None, None, None))
+
+
+def test_tangent_mode_switch_is_checked():
+    """bmc_set_tangent_mode takes BMC_TANGENTS_AUTO or BMC_TANGENTS_FORWARD and refuses anything else."""
+    from bmc_b200 import settings
+    L = _lib.lib()
+    assert L.bmc_set_tangent_mode(7) != 0
+    assert L.bmc_set_tangent_mode(_lib.TANGENTS_FORWARD) == 0
+    assert L.bmc_set_tangent_mode(_lib.TANGENTS_AUTO) == 0
+    with pytest.raises(ValueError):
+        settings.use_tangents("reverse")
+    assert settings.use_tangents("forward") == "forward" and settings.tangent_mode() == "forward"
+    assert settings.use_tangents("auto") == "auto"
