@@ -12,9 +12,12 @@
 //
 // exp(X) and H come together from the dual scaling and squaring of X + eps E, E = v lam^T: the Horner
 // recurrence of exp(X / 2^s) with the tangent direction E / 2^s, then s squarings of the pair
-// [T, H] -> [T T, T H + H T] (exp(2Y + 2 eps F) = exp(Y + eps F)^2). As on the dense path of the chain
-// kernel, a group of lanes takes one chain, lane j holding column j of T and of H; T's last row is e_N^T
-// (the augmented row) and is not stored, H's is (E has a last row: v_N lam^T = lam^T).
+// [T, H] -> [T T, T H + H T] (exp(2Y + 2 eps F) = exp(Y + eps F)^2). A group of lanes takes one chain,
+// lane j < N holding column j of T and of H. T's last row is e_N^T (the augmented row) and is not
+// stored; H's is (E has a last row: v_N lam^T = lam^T). The augmented column of T, phi = T[0:N, N], is
+// kept apart in shared memory, lane i updating row i (phi <- T phi + phi), and the augmented column
+// of H is never formed: it enters column j < N only through T[N][j] = 0, and no tangent reads it. So
+// a chain takes N lanes, not N + 1: with four CEST pools (N = 16) two chains share a warp.
 //
 // The tangent coefficient sets dX_p = [dA_p dC_p; 0 0] dt come from the chain kernel's own coefficient
 // code with a one-direction dual number, lane p of the group computing set p; lane i then forms
@@ -25,29 +28,40 @@
 
 namespace bmc {
 
+// lanes per chain: the state columns, rounded up to a divisor of the warp
+template <int NC>
+struct AdjGroup {
+    static constexpr int N = Layout<NC>::N;
+    static constexpr int GS = N <= 4 ? 4 : (N <= 8 ? 8 : (N <= 16 ? 16 : 32));
+    static constexpr int G = 32 / GS;
+    static constexpr int LD = (N + 1) | 1;             // odd column stride; H's columns have N + 1 rows
+    static constexpr int PHI_LANE = N < GS ? N : 0;    // the lane that forms phi's Horner recurrence
+};
+
 template <int NC>
 struct AdjSlotBody {
     static constexpr int N = Layout<NC>::N;
-    static constexpr int NA = N + 1;
-    static constexpr int LD = DenseGroup<NC>::LD;
+    static constexpr int LD = AdjGroup<NC>::LD;
     using K = StepCoef<NC, Dn<double, 0>>;
     K coef;                                   // the owner's coefficients times h = dt / 2^s
     double cw, cm, cc[NC > 0 ? NC : 1];       // ... and its constant column C h
-    double T[NA * LD];                        // column-major: column j at [j * LD], rows 0 .. N - 1
-    double H[NA * LD];                        // rows 0 .. N
-    double v[NA];                             // [M0; 1]
+    double T[N * LD];                         // column-major: column j at [j * LD], rows 0 .. N - 1
+    double H[N * LD];                         // rows 0 .. N
+    double phi[2][N];                         // T's augmented column, one buffer read while the other is written
+    double v[N + 1];                          // [M0; 1]
     K dk[kMaxT];                              // per tangent: the coefficients' derivative times dt
     double dcw[kMaxT], dcm[kMaxT], dcc[kMaxT][NC > 0 ? NC : 1];   // ... and C's
     double res[kMaxT + 1];                    // the group's sums: tangents, then z
     EvRec<double> rec;
-    double g0, scale;                         // the owner's MT lineshape value; 2^-s
+    double g0, gd[3], scale;                  // the owner's MT lineshape and its partial derivatives in
+                                              // (offset, T2, bridge width); 2^-s
     int s, vox;
 };
 
 template <int NC>
 struct AdjSlot : AdjSlotBody<NC> {
     static constexpr size_t kBody = sizeof(AdjSlotBody<NC>);
-    static constexpr size_t kTarget = (128 / DenseGroup<NC>::G) % 128;
+    static constexpr size_t kTarget = (128 / AdjGroup<NC>::G) % 128;
     static constexpr size_t kPad = (kTarget + 128 - kBody % 128) % 128;
     char pad[kPad == 0 ? 128 : kPad];
 };
@@ -98,10 +112,9 @@ struct Adjoint {
     using K = StepCoef<NC, D0>;
     using SL = AdjSlot<NC>;
     static constexpr int N = Layout<NC>::N;
-    static constexpr int NA = N + 1;
-    static constexpr int GS = DenseGroup<NC>::GS;
-    static constexpr int G = DenseGroup<NC>::G;
-    static constexpr int LD = DenseGroup<NC>::LD;
+    static constexpr int GS = AdjGroup<NC>::GS;
+    static constexpr int G = AdjGroup<NC>::G;
+    static constexpr int LD = AdjGroup<NC>::LD;
 
     static __device__ __forceinline__ double get(const S& x, int q) {
         double r = 0.0;
@@ -137,14 +150,12 @@ struct Adjoint {
         ChainConst<NC, D1> cp;
         C1::load_const(a, sl->vox, node, cp, p);
         const EvRec<double>& rec = sl->rec;
+        // the lineshape's derivative by the chain rule through its three arguments (their partials were
+        // formed once per chain, by the chain's own thread)
         D1 g = dconst<double, 1>(sl->g0);
         if (cp.mt_on && cp.ls != 0 && rec.w1 != 0.0) {
             const D1 offmt = (rec.wf - cp.dw0) - cp.dwmt;
-            // a tangent that moves neither the MT offset nor T2 leaves the lineshape's value: its
-            // derivative is 0 exactly, as the dual evaluation would give
-            if (offmt.d[0] != 0.0 || cp.t2mt.d[0] != 0.0 || cp.w0sl.d[0] != 0.0)
-                g = cp.ls == 1 ? lorentzian<double, 1>(offmt, cp.t2mt)
-                               : super_lorentzian<double, 1>(offmt, cp.t2mt, cp.w0sl);
+            g.d[0] = fma(sl->gd[0], offmt.d[0], fma(sl->gd[1], cp.t2mt.d[0], sl->gd[2] * cp.w0sl.d[0]));
         }
         StepCoef<NC, D1> sp;
         C1::event_coef(cp, rec, g, sp);
@@ -185,7 +196,7 @@ adjoint_kernel(const ChainArgs a, const int* __restrict__ row_ev, int n_tan, con
     using C0 = Chain<NC, double, 0>;
     using S = State<NC, D0>;
     using SL = AdjSlot<NC>;
-    constexpr int N = A::N, NA = A::NA, GS = A::GS, G = A::G, LD = A::LD;
+    constexpr int N = A::N, GS = A::GS, G = A::G, LD = A::LD, PHI_LANE = AdjGroup<NC>::PHI_LANE;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SL* slots = reinterpret_cast<SL*>(smem_raw) + (threadIdx.x >> 5) * G;
     const TaylorTable& tt = *ttab;
@@ -206,13 +217,18 @@ adjoint_kernel(const ChainArgs a, const int* __restrict__ row_ev, int n_tan, con
     for (int node = 0; node < a.n_nodes; ++node) {
         // this chain's event: coefficients, norm, squarings
         int s = 0;
-        double h = 0.0, g0 = 0.0;
+        Dn<double, 3> g3 = dconst<double, 3>(0.0);
         ChainConst<NC, D0> cc;
         C0::load_const(a, v, node, cc);
         if (cc.mt_on && cc.ls != 0 && rec.w1 != 0.0) {
-            const D0 offmt = (rec.wf - cc.dw0) - cc.dwmt;
-            g0 = (cc.ls == 1 ? lorentzian<double, 0>(offmt, cc.t2mt) : super_lorentzian<double, 0>(offmt, cc.t2mt, cc.w0sl)).v;
+            Dn<double, 3> off3 = dconst<double, 3>(((rec.wf - cc.dw0) - cc.dwmt).v);
+            Dn<double, 3> t23 = dconst<double, 3>(cc.t2mt.v), w03 = dconst<double, 3>(cc.w0sl.v);
+            off3.d[0] = 1.0;
+            t23.d[1] = 1.0;
+            w03.d[2] = 1.0;
+            g3 = cc.ls == 1 ? lorentzian<double, 3>(off3, t23) : super_lorentzian<double, 3>(off3, t23, w03);
         }
+        const double g0 = g3.v;
         StepCoef<NC, D0> sc;
         C0::event_coef(cc, rec, dconst<double, 0>(g0), sc);
         double nu = rec.dt * C0::coef_norm(sc, cc);
@@ -227,7 +243,7 @@ adjoint_kernel(const ChainArgs a, const int* __restrict__ row_ev, int n_tan, con
             capped = true;
             if (act) atomicOr(a.status, 2);
         }
-        h = ldexp(rec.dt, -s);
+        const double h = ldexp(rec.dt, -s);
 
         unsigned need = __ballot_sync(kFull, act);
         while (need) {
@@ -254,32 +270,35 @@ adjoint_kernel(const ChainArgs a, const int* __restrict__ row_ev, int n_tan, con
                 sl->v[N] = 1.0;
                 sl->rec = rec;
                 sl->g0 = g0;
+                sl->gd[0] = g3.d[0];
+                sl->gd[1] = g3.d[1];
+                sl->gd[2] = g3.d[2];
                 sl->scale = ldexp(1.0, -s);
                 sl->s = s;
                 sl->vox = v;
                 if (a.work) {
-                    wk1 += unsigned(NA * tt.dense_m);
+                    wk1 += unsigned((N + 1) * tt.dense_m);
                     wk2 += unsigned(s);
                 }
             }
             __syncwarp();
             SL* sl = &slots[grp];
             const bool have = grp_owner >= 0;
-            if (have && gl < n_tan) A::tangent_set(a, sl, node, gl);
-            const bool work = have && gl < NA;
+            if (have)
+                for (int p = gl; p < n_tan; p += GS) A::tangent_set(a, sl, node, p);
+            const bool work = have && gl < N;
             const int s_g = have ? sl->s : 0;
             const int smax = (int)__reduce_max_sync(kFull, (unsigned)s_g);
             // column gl of exp(X / 2^s) and of its derivative along E / 2^s: Horner, T = I + X T / k
             S cv, cd;
             double cdN = 0.0;
-            const double caug = gl == N ? 1.0 : 0.0;
             A::unit(cv, gl);
             A::unit(cd, -1);
             if (work) {
                 const double e2 = sl->scale;
                 for (int k = tt.dense_m; k >= 1; --k) {
                     S yv, yd;
-                    A::op(sl, cv, caug, yv);
+                    C0::template matvec<false>(sl->coef, cv, yv);
                     A::op(sl, cd, cdN, yd);
                     const double dot = e2 * A::get(cv, a.mz);     // (E / 2^s) column: v (lam . col) / 2^s
                     const double ik = tt.inv_k[k];
@@ -291,8 +310,22 @@ adjoint_kernel(const ChainArgs a, const int* __restrict__ row_ev, int n_tan, con
                     cdN = ik * dot;
                 }
             }
+            // the augmented column: [phi; 1] <- e_N + X [phi; 1] / k
+            if (have && gl == PHI_LANE) {
+                S ph;
+                A::unit(ph, -1);
+                for (int k = tt.dense_m; k >= 1; --k) {
+                    S y;
+                    A::op(sl, ph, 1.0, y);
+                    const double ik = tt.inv_k[k];
+#pragma unroll
+                    for (int q = 0; q < N; ++q) C0::at(ph, q).v = ik * C0::at(y, q).v;
+                }
+#pragma unroll
+                for (int q = 0; q < N; ++q) sl->phi[0][q] = C0::at(ph, q).v;
+            }
             __syncwarp();
-            // s squarings: [T, H] <- [T T, T H + H T]
+            // s squarings: [T, H] <- [T T, T H + H T], phi <- T phi + phi
             for (int q = 0; q < smax; ++q) {
                 const bool sq = work && q < s_g;
                 if (sq) {
@@ -305,15 +338,14 @@ adjoint_kernel(const ChainArgs a, const int* __restrict__ row_ev, int n_tan, con
                 }
                 __syncwarp();
                 if (sq) {
+                    const double* ph = sl->phi[q & 1];
                     S nv, nd;
-                    double ndN = cdN;
+                    double ndN = cdN, pj = ph[gl];
 #pragma unroll
                     for (int i = 0; i < N; ++i) {
-                        const double t_aug = sl->T[N * LD + i], h_aug = sl->H[N * LD + i];
-                        C0::at(nv, i).v = caug * t_aug;
-                        C0::at(nd, i).v = fma(t_aug, cdN, caug * h_aug);
+                        C0::at(nv, i).v = 0.0;
+                        C0::at(nd, i).v = ph[i] * cdN;
                     }
-                    ndN = fma(caug, sl->H[N * LD + N], ndN);
 #pragma unroll
                     for (int l = 0; l < N; ++l) {
                         const double wv = C0::at(cv, l).v, wd = C0::at(cd, l).v;
@@ -324,26 +356,29 @@ adjoint_kernel(const ChainArgs a, const int* __restrict__ row_ev, int n_tan, con
                             C0::at(nd, i).v = fma(t, wd, fma(sl->H[l * LD + i], wv, C0::at(nd, i).v));
                         }
                         ndN = fma(sl->H[l * LD + N], wv, ndN);
+                        pj = fma(sl->T[l * LD + gl], ph[l], pj);
                     }
+                    sl->phi[(q + 1) & 1][gl] = pj;
                     cv = nv;
                     cd = nd;
                     cdN = ndN;
                 }
                 __syncwarp();
             }
-            // z = sum_j (exp(X)^T lam)_j v_j, and per tangent tr(dX_p H) + (exp(X)^T lam) . dv_p
+            // z = sum_j (exp(X)^T lam)_j v_j (phi[mz] for j = N), and per tangent
+            // tr(dX_p H) + (exp(X)^T lam) . dv_p
             const double u = work ? A::get(cv, a.mz) : 0.0;
             const double zsum = group_sum<GS>(work ? u * sl->v[gl] : 0.0);
             for (int p = 0; p < n_tan; ++p) {
                 double gp = 0.0;
-                if (work && gl < N) {
+                if (work) {
                     gp = A::dop_row(sl, p, cd, cdN, gl);
                     if (a.dm0) gp = fma(u, a.dm0[((size_t)p * a.n_vox + sl->vox) * N + gl], gp);
                 }
                 gp = group_sum<GS>(gp);
                 if (have && gl == 0) sl->res[p] = gp;
             }
-            if (have && gl == 0) sl->res[kMaxT] = zsum;
+            if (have && gl == 0) sl->res[kMaxT] = zsum + sl->phi[s_g & 1][a.mz];
             __syncwarp();
             if (my_slot >= 0) {
                 const SL* ms = &slots[my_slot];

@@ -303,7 +303,7 @@ std::atomic<int> g_tangent_mode{BMC_TANGENTS_AUTO};
 
 template <int NC>
 bmc_status launch_adjoint(const ChainArgs& a, const int* row_ev, int n_tan, const TaylorTable* tt, cudaStream_t st) {
-    const size_t smem = kAdjWarps * DenseGroup<NC>::G * sizeof(AdjSlot<NC>);
+    const size_t smem = kAdjWarps * AdjGroup<NC>::G * sizeof(AdjSlot<NC>);
     static std::atomic<unsigned long long> configured{0};
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
