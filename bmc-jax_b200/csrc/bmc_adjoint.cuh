@@ -188,8 +188,13 @@ struct Adjoint {
     }
 };
 
-template <int NC>
-__global__ void __launch_bounds__(32 * kAdjWarps, 2)
+// kTan false: z only (the same layout and arithmetic without H), for the LM's trial points. Blocks per SM
+// the register allocation aims at (a build may set BMC_ADJ_PRIMAL_BLOCKS for a sweep).
+#ifndef BMC_ADJ_PRIMAL_BLOCKS
+#define BMC_ADJ_PRIMAL_BLOCKS 2
+#endif
+template <int NC, bool kTan>
+__global__ void __launch_bounds__(32 * kAdjWarps, kTan ? 2 : BMC_ADJ_PRIMAL_BLOCKS)
 adjoint_kernel(const ChainArgs a, const int* __restrict__ row_ev, int n_tan, const TaylorTable* __restrict__ ttab) {
     using A = Adjoint<NC>;
     using D0 = Dn<double, 0>;
@@ -220,7 +225,11 @@ adjoint_kernel(const ChainArgs a, const int* __restrict__ row_ev, int n_tan, con
         Dn<double, 3> g3 = dconst<double, 3>(0.0);
         ChainConst<NC, D0> cc;
         C0::load_const(a, v, node, cc);
-        if (cc.mt_on && cc.ls != 0 && rec.w1 != 0.0) {
+        if (!kTan && cc.mt_on && cc.ls != 0 && rec.w1 != 0.0) {
+            const D0 offmt = (rec.wf - cc.dw0) - cc.dwmt;
+            g3.v = (cc.ls == 1 ? lorentzian<double, 0>(offmt, cc.t2mt)
+                               : super_lorentzian<double, 0>(offmt, cc.t2mt, cc.w0sl)).v;
+        } else if (kTan && cc.mt_on && cc.ls != 0 && rec.w1 != 0.0) {
             Dn<double, 3> off3 = dconst<double, 3>(((rec.wf - cc.dw0) - cc.dwmt).v);
             Dn<double, 3> t23 = dconst<double, 3>(cc.t2mt.v), w03 = dconst<double, 3>(cc.w0sl.v);
             off3.d[0] = 1.0;
@@ -284,8 +293,10 @@ adjoint_kernel(const ChainArgs a, const int* __restrict__ row_ev, int n_tan, con
             __syncwarp();
             SL* sl = &slots[grp];
             const bool have = grp_owner >= 0;
-            if (have)
-                for (int p = gl; p < n_tan; p += GS) A::tangent_set(a, sl, node, p);
+            if constexpr (kTan) {
+                if (have)
+                    for (int p = gl; p < n_tan; p += GS) A::tangent_set(a, sl, node, p);
+            }
             const bool work = have && gl < N;
             const int s_g = have ? sl->s : 0;
             const int smax = (int)__reduce_max_sync(kFull, (unsigned)s_g);
@@ -297,17 +308,19 @@ adjoint_kernel(const ChainArgs a, const int* __restrict__ row_ev, int n_tan, con
             if (work) {
                 const double e2 = sl->scale;
                 for (int k = tt.dense_m; k >= 1; --k) {
-                    S yv, yd;
+                    S yv;
                     C0::template matvec<false>(sl->coef, cv, yv);
-                    A::op(sl, cd, cdN, yd);
-                    const double dot = e2 * A::get(cv, a.mz);     // (E / 2^s) column: v (lam . col) / 2^s
                     const double ik = tt.inv_k[k];
+                    if constexpr (kTan) {
+                        S yd;
+                        A::op(sl, cd, cdN, yd);
+                        const double dot = e2 * A::get(cv, a.mz);     // (E / 2^s) column: v (lam . col) / 2^s
 #pragma unroll
-                    for (int q = 0; q < N; ++q) {
-                        C0::at(cv, q).v = (q == gl ? 1.0 : 0.0) + ik * C0::at(yv, q).v;
-                        C0::at(cd, q).v = ik * fma(dot, sl->v[q], C0::at(yd, q).v);
+                        for (int q = 0; q < N; ++q) C0::at(cd, q).v = ik * fma(dot, sl->v[q], C0::at(yd, q).v);
+                        cdN = ik * dot;
                     }
-                    cdN = ik * dot;
+#pragma unroll
+                    for (int q = 0; q < N; ++q) C0::at(cv, q).v = (q == gl ? 1.0 : 0.0) + ik * C0::at(yv, q).v;
                 }
             }
             // the augmented column: [phi; 1] <- e_N + X [phi; 1] / k
@@ -332,9 +345,9 @@ adjoint_kernel(const ChainArgs a, const int* __restrict__ row_ev, int n_tan, con
 #pragma unroll
                     for (int i = 0; i < N; ++i) {
                         sl->T[gl * LD + i] = C0::at(cv, i).v;
-                        sl->H[gl * LD + i] = C0::at(cd, i).v;
+                        if constexpr (kTan) sl->H[gl * LD + i] = C0::at(cd, i).v;
                     }
-                    sl->H[gl * LD + N] = cdN;
+                    if constexpr (kTan) sl->H[gl * LD + N] = cdN;
                 }
                 __syncwarp();
                 if (sq) {
@@ -344,24 +357,27 @@ adjoint_kernel(const ChainArgs a, const int* __restrict__ row_ev, int n_tan, con
 #pragma unroll
                     for (int i = 0; i < N; ++i) {
                         C0::at(nv, i).v = 0.0;
-                        C0::at(nd, i).v = ph[i] * cdN;
+                        if constexpr (kTan) C0::at(nd, i).v = ph[i] * cdN;
                     }
 #pragma unroll
                     for (int l = 0; l < N; ++l) {
-                        const double wv = C0::at(cv, l).v, wd = C0::at(cd, l).v;
+                        const double wv = C0::at(cv, l).v;
 #pragma unroll
                         for (int i = 0; i < N; ++i) {
                             const double t = sl->T[l * LD + i];
                             C0::at(nv, i).v = fma(t, wv, C0::at(nv, i).v);
-                            C0::at(nd, i).v = fma(t, wd, fma(sl->H[l * LD + i], wv, C0::at(nd, i).v));
+                            if constexpr (kTan)
+                                C0::at(nd, i).v = fma(t, C0::at(cd, l).v, fma(sl->H[l * LD + i], wv, C0::at(nd, i).v));
                         }
-                        ndN = fma(sl->H[l * LD + N], wv, ndN);
+                        if constexpr (kTan) ndN = fma(sl->H[l * LD + N], wv, ndN);
                         pj = fma(sl->T[l * LD + gl], ph[l], pj);
                     }
                     sl->phi[(q + 1) & 1][gl] = pj;
                     cv = nv;
-                    cd = nd;
-                    cdN = ndN;
+                    if constexpr (kTan) {
+                        cd = nd;
+                        cdN = ndN;
+                    }
                 }
                 __syncwarp();
             }
@@ -369,7 +385,7 @@ adjoint_kernel(const ChainArgs a, const int* __restrict__ row_ev, int n_tan, con
             // tr(dX_p H) + (exp(X)^T lam) . dv_p
             const double u = work ? A::get(cv, a.mz) : 0.0;
             const double zsum = group_sum<GS>(work ? u * sl->v[gl] : 0.0);
-            for (int p = 0; p < n_tan; ++p) {
+            for (int p = 0; p < (kTan ? n_tan : 0); ++p) {
                 double gp = 0.0;
                 if (work) {
                     gp = A::dop_row(sl, p, cd, cdN, gl);
@@ -385,7 +401,7 @@ adjoint_kernel(const ChainArgs a, const int* __restrict__ row_ev, int n_tan, con
                 const double wgt = a.n_nodes > 1 ? a.w[node] : 1.0;
                 const double z = capped ? NAN : ms->res[kMaxT];
                 a.out[ch] = (node ? a.out[ch] : 0.0) + wgt * z;
-                for (int p = 0; p < n_tan; ++p) {
+                for (int p = 0; p < (kTan ? n_tan : 0); ++p) {
                     double* jp = a.jout + ((size_t)p * a.n_vox + v) * a.n_off + o;
                     *jp = (node ? *jp : 0.0) + wgt * (capped ? NAN : ms->res[p]);
                 }

@@ -301,21 +301,22 @@ bmc_status launch_chain(const ChainArgs& a, const TaylorTable* tt, cudaStream_t 
 // Tangent mode (bmc_set_tangent_mode): BMC_TANGENTS_AUTO takes the adjoint kernel where it applies.
 std::atomic<int> g_tangent_mode{BMC_TANGENTS_AUTO};
 
-template <int NC>
+template <int NC, bool kTan = true>
 bmc_status launch_adjoint(const ChainArgs& a, const int* row_ev, int n_tan, const TaylorTable* tt, cudaStream_t st) {
     const size_t smem = kAdjWarps * AdjGroup<NC>::G * sizeof(AdjSlot<NC>);
     static std::atomic<unsigned long long> configured{0};
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
     if (dev >= 64 || !((configured.load(std::memory_order_acquire) >> dev) & 1ull)) {
-        CUDA_TRY(cudaFuncSetAttribute(adjoint_kernel<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CUDA_TRY(cudaFuncSetAttribute(adjoint_kernel<NC, kTan>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
         if (dev < 64) configured.fetch_or(1ull << dev, std::memory_order_acq_rel);
     }
     const long long nch = (long long)a.n_vox * a.n_off;
     const long long blocks = (nch + kAdjWarps * 32 - 1) / (kAdjWarps * 32);
     if (blocks > 0x7fffffffLL) return fail(BMC_ERR_INVALID, "%lld chains exceed one launch", nch);
     if (blocks == 0) return BMC_OK;
-    adjoint_kernel<NC><<<(unsigned)blocks, kAdjWarps * 32, smem, st>>>(a, row_ev, n_tan, tt);
+    adjoint_kernel<NC, kTan><<<(unsigned)blocks, kAdjWarps * 32, smem, st>>>(a, row_ev, n_tan, tt);
     CUDA_TRY(cudaGetLastError());
     return BMC_OK;
 }
@@ -634,7 +635,10 @@ struct Impl {
             CUDA_TRY(cudaGetLastError());
             ChainArgs at = a;
             at.params = pt; at.m0 = m0t; at.sigma = sp ? sgt : nullptr; at.out = zt;
-            if ((s = launch_chain<NC, double, 0>(at, tt, st)) != BMC_OK) return s;
+            // the trial point's Z: with the adjoint tangents, the same dense layout without H
+            if ((s = adj ? launch_adjoint<NC, false>(at, row_ev, 0, tt, st) : launch_chain<NC, double, 0>(at, tt, st)) !=
+                BMC_OK)
+                return s;
             lm_accept_kernel<<<wb, 128, 0, st>>>(nv, no, fs->n_points_skip, P, it, fs->n_iter, zt, zm, cost, xt, x,
                                                  lam, need, cost_traj, x_traj);
             CUDA_TRY(cudaGetLastError());
