@@ -34,9 +34,22 @@ struct AdjGroup {
     static constexpr int N = Layout<NC>::N;
     static constexpr int GS = N <= 4 ? 4 : (N <= 8 ? 8 : (N <= 16 ? 16 : 32));
     static constexpr int G = 32 / GS;
-    static constexpr int LD = (N + 1) | 1;             // odd column stride; H's columns have N + 1 rows
+    // N = 16 (four CEST pools): the squarings on the FP64 tensor cores (mma.sync m8n8k4, 2 x 2 tiles of
+    // 8 x 8), the warp taking its two chains in turn. Column stride 20 (4 mod 16 doubles): the 32 lanes
+    // of a fragment load, (row, col) = (g, t) or (t, g) with g < 8, t < 4, hit each 8-byte bank twice.
+    // Otherwise the lanes' own FMAs, odd stride (H's columns have N + 1 rows).
+    static constexpr bool kMma = N == 16;
+    static constexpr int LD = kMma ? 20 : ((N + 1) | 1);
     static constexpr int PHI_LANE = N < GS ? N : 0;    // the lane that forms phi's Horner recurrence
 };
+
+// D += A B for one 8x8x4 tile (row-major A, column-major B; lane l holds A[l / 4][l % 4], B[l % 4][l / 4]
+// and D[l / 4][2 (l % 4) + 0, 1])
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+        : "+d"(d0), "+d"(d1)
+        : "d"(a), "d"(b));
+}
 
 template <int NC>
 struct AdjSlotBody {
@@ -185,6 +198,96 @@ struct Adjoint {
     static __device__ __forceinline__ void unit(S& x, int j) {
 #pragma unroll
         for (int q = 0; q < N; ++q) C0::at(x, q).v = q == j ? 1.0 : 0.0;
+    }
+
+    // One squaring of a slot's pair, in place, by the whole warp (N = 16):
+    //   T <- T T,  H[0:N] <- T H[0:N] + H[0:N] T + phi h^T,  h <- h + h T,  phi <- T phi + phi
+    // (h = H's augmented row). The rank-one term is a fifth k-step whose A column is phi and whose B row is
+    // h; lanes 0-15 form h, lanes 16-31 phi. Everything is read before the warp synchronises and writes.
+    template <bool kTan>
+    static __device__ __forceinline__ void mma_square(SL* sl, int lane) {
+        static_assert(N == 16, "tiles of 8 x 8 over a 16 x 16 matrix");
+        const int g = lane >> 2, t = lane & 3;
+        double* T = sl->T;
+        double* H = sl->H;
+        double* ph = sl->phi[0];
+        double aT[2][4], bT[4][2], cT[2][2][2];
+#pragma unroll
+        for (int I = 0; I < 2; ++I)
+#pragma unroll
+            for (int K = 0; K < 4; ++K) aT[I][K] = T[(4 * K + t) * LD + 8 * I + g];
+#pragma unroll
+        for (int K = 0; K < 4; ++K)
+#pragma unroll
+            for (int J = 0; J < 2; ++J) bT[K][J] = T[(8 * J + g) * LD + 4 * K + t];
+#pragma unroll
+        for (int I = 0; I < 2; ++I)
+#pragma unroll
+            for (int J = 0; J < 2; ++J) {
+                cT[I][J][0] = 0.0;
+                cT[I][J][1] = 0.0;
+#pragma unroll
+                for (int K = 0; K < 4; ++K) dmma(cT[I][J][0], cT[I][J][1], aT[I][K], bT[K][J]);
+            }
+        double cH[2][2][2];
+        if constexpr (kTan) {
+            double aH[2][4], bH[4][2], aP[2], bP[2];
+#pragma unroll
+            for (int I = 0; I < 2; ++I) {
+#pragma unroll
+                for (int K = 0; K < 4; ++K) aH[I][K] = H[(4 * K + t) * LD + 8 * I + g];
+                aP[I] = t == 0 ? ph[8 * I + g] : 0.0;
+            }
+#pragma unroll
+            for (int J = 0; J < 2; ++J) {
+#pragma unroll
+                for (int K = 0; K < 4; ++K) bH[K][J] = H[(8 * J + g) * LD + 4 * K + t];
+                bP[J] = t == 0 ? H[(8 * J + g) * LD + N] : 0.0;
+            }
+#pragma unroll
+            for (int I = 0; I < 2; ++I)
+#pragma unroll
+                for (int J = 0; J < 2; ++J) {
+                    cH[I][J][0] = 0.0;
+                    cH[I][J][1] = 0.0;
+#pragma unroll
+                    for (int K = 0; K < 4; ++K) {
+                        dmma(cH[I][J][0], cH[I][J][1], aT[I][K], bH[K][J]);
+                        dmma(cH[I][J][0], cH[I][J][1], aH[I][K], bT[K][J]);
+                    }
+                    dmma(cH[I][J][0], cH[I][J][1], aP[I], bP[J]);
+                }
+        }
+        // h (lanes 0-15, one column each) and phi (lanes 16-31, one row each)
+        double vec = 0.0;
+        if (lane < N) {
+            if constexpr (kTan) {
+                vec = H[lane * LD + N];
+#pragma unroll
+                for (int l = 0; l < N; ++l) vec = fma(H[l * LD + N], T[lane * LD + l], vec);
+            }
+        } else {
+            const int i = lane - N;
+            vec = ph[i];
+#pragma unroll
+            for (int l = 0; l < N; ++l) vec = fma(T[l * LD + i], ph[l], vec);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int I = 0; I < 2; ++I)
+#pragma unroll
+            for (int J = 0; J < 2; ++J)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    T[(8 * J + 2 * t + e) * LD + 8 * I + g] = cT[I][J][e];
+                    if constexpr (kTan) H[(8 * J + 2 * t + e) * LD + 8 * I + g] = cH[I][J][e];
+                }
+        if (lane < N) {
+            if constexpr (kTan) H[lane * LD + N] = vec;
+        } else {
+            ph[lane - N] = vec;
+        }
+        __syncwarp();
     }
 };
 
@@ -339,9 +442,8 @@ adjoint_kernel(const ChainArgs a, const int* __restrict__ row_ev, int n_tan, con
             }
             __syncwarp();
             // s squarings: [T, H] <- [T T, T H + H T], phi <- T phi + phi
-            for (int q = 0; q < smax; ++q) {
-                const bool sq = work && q < s_g;
-                if (sq) {
+            if constexpr (AdjGroup<NC>::kMma) {
+                if (work) {
 #pragma unroll
                     for (int i = 0; i < N; ++i) {
                         sl->T[gl * LD + i] = C0::at(cv, i).v;
@@ -350,36 +452,64 @@ adjoint_kernel(const ChainArgs a, const int* __restrict__ row_ev, int n_tan, con
                     if constexpr (kTan) sl->H[gl * LD + N] = cdN;
                 }
                 __syncwarp();
-                if (sq) {
-                    const double* ph = sl->phi[q & 1];
-                    S nv, nd;
-                    double ndN = cdN, pj = ph[gl];
+                for (int q = 0; q < smax; ++q) {
 #pragma unroll
-                    for (int i = 0; i < N; ++i) {
-                        C0::at(nv, i).v = 0.0;
-                        if constexpr (kTan) C0::at(nd, i).v = ph[i] * cdN;
-                    }
-#pragma unroll
-                    for (int l = 0; l < N; ++l) {
-                        const double wv = C0::at(cv, l).v;
-#pragma unroll
-                        for (int i = 0; i < N; ++i) {
-                            const double t = sl->T[l * LD + i];
-                            C0::at(nv, i).v = fma(t, wv, C0::at(nv, i).v);
-                            if constexpr (kTan)
-                                C0::at(nd, i).v = fma(t, C0::at(cd, l).v, fma(sl->H[l * LD + i], wv, C0::at(nd, i).v));
-                        }
-                        if constexpr (kTan) ndN = fma(sl->H[l * LD + N], wv, ndN);
-                        pj = fma(sl->T[l * LD + gl], ph[l], pj);
-                    }
-                    sl->phi[(q + 1) & 1][gl] = pj;
-                    cv = nv;
-                    if constexpr (kTan) {
-                        cd = nd;
-                        cdN = ndN;
+                    for (int c = 0; c < G; ++c) {
+                        const int s_c = __shfl_sync(kFull, s_g, c * GS);
+                        if (q < s_c) A::template mma_square<kTan>(&slots[c], lane);
                     }
                 }
-                __syncwarp();
+                if (work) {
+#pragma unroll
+                    for (int i = 0; i < N; ++i) {
+                        C0::at(cv, i).v = sl->T[gl * LD + i];
+                        if constexpr (kTan) C0::at(cd, i).v = sl->H[gl * LD + i];
+                    }
+                    if constexpr (kTan) cdN = sl->H[gl * LD + N];
+                }
+            } else {
+                for (int q = 0; q < smax; ++q) {
+                    const bool sq = work && q < s_g;
+                    if (sq) {
+#pragma unroll
+                        for (int i = 0; i < N; ++i) {
+                            sl->T[gl * LD + i] = C0::at(cv, i).v;
+                            if constexpr (kTan) sl->H[gl * LD + i] = C0::at(cd, i).v;
+                        }
+                        if constexpr (kTan) sl->H[gl * LD + N] = cdN;
+                    }
+                    __syncwarp();
+                    if (sq) {
+                        const double* ph = sl->phi[q & 1];
+                        S nv, nd;
+                        double ndN = cdN, pj = ph[gl];
+#pragma unroll
+                        for (int i = 0; i < N; ++i) {
+                            C0::at(nv, i).v = 0.0;
+                            if constexpr (kTan) C0::at(nd, i).v = ph[i] * cdN;
+                        }
+#pragma unroll
+                        for (int l = 0; l < N; ++l) {
+                            const double wv = C0::at(cv, l).v;
+#pragma unroll
+                            for (int i = 0; i < N; ++i) {
+                                const double t = sl->T[l * LD + i];
+                                C0::at(nv, i).v = fma(t, wv, C0::at(nv, i).v);
+                                if constexpr (kTan)
+                                    C0::at(nd, i).v = fma(t, C0::at(cd, l).v, fma(sl->H[l * LD + i], wv, C0::at(nd, i).v));
+                            }
+                            if constexpr (kTan) ndN = fma(sl->H[l * LD + N], wv, ndN);
+                            pj = fma(sl->T[l * LD + gl], ph[l], pj);
+                        }
+                        sl->phi[(q + 1) & 1][gl] = pj;
+                        cv = nv;
+                        if constexpr (kTan) {
+                            cd = nd;
+                            cdN = ndN;
+                        }
+                    }
+                    __syncwarp();
+                }
             }
             // z = sum_j (exp(X)^T lam)_j v_j (phi[mz] for j = N), and per tangent
             // tr(dX_p H) + (exp(X)^T lam) . dv_p
@@ -394,7 +524,7 @@ adjoint_kernel(const ChainArgs a, const int* __restrict__ row_ev, int n_tan, con
                 gp = group_sum<GS>(gp);
                 if (have && gl == 0) sl->res[p] = gp;
             }
-            if (have && gl == 0) sl->res[kMaxT] = zsum + sl->phi[s_g & 1][a.mz];
+            if (have && gl == 0) sl->res[kMaxT] = zsum + sl->phi[AdjGroup<NC>::kMma ? 0 : (s_g & 1)][a.mz];
             __syncwarp();
             if (my_slot >= 0) {
                 const SL* ms = &slots[my_slot];
