@@ -692,36 +692,49 @@ def mlp_roofline(n_in, n_out, n_hidden=256, n_layers=3, batch=4096, steps=50, in
     t = torch.rand((batch, n_out), generator=g, device="cuda")
     xi = torch.rand((infer_batch, n_in), generator=g, device="cuda")
 
+    d_step = torch.zeros(1, dtype=torch.int32, device="cuda")
+
     def step():
         net.forward(x, keep=True)
         net.backward(t)
-        net.adam(1e-4)
+        net.adam_dev(d_step, 1e-4)
 
     for _ in range(5):
         step()
     net.forward(xi)
+    graph = torch.cuda.CUDAGraph()                 # what MLP.train replays
+    with torch.cuda.graph(graph):
+        step()
+    graph.replay()
     torch.cuda.synchronize()
-    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0, e1, e2, e3 = (torch.cuda.Event(enable_timing=True) for _ in range(4))
     e0.record()
     for _ in range(steps):
         step()
     e1.record()
-    net.forward(xi)
+    for _ in range(steps):
+        graph.replay()
     e2.record()
-    e2.synchronize()
+    net.forward(xi)
+    e3.record()
+    e3.synchronize()
+    del graph
     F = 2.0 * (n_in * n_hidden + (n_layers - 1) * n_hidden ** 2 + n_hidden * n_out)
-    train_tf = (3 * F - 2.0 * n_in * n_hidden) * batch * steps / (e0.elapsed_time(e1) * 1e-3) / 1e12
-    infer_tf = F * infer_batch / (e1.elapsed_time(e2) * 1e-3) / 1e12
+    step_flops = (3 * F - 2.0 * n_in * n_hidden) * batch
+    train_ms = e1.elapsed_time(e2) / steps
+    train_tf = step_flops / (train_ms * 1e-3) / 1e12
+    infer_tf = F * infer_batch / (e2.elapsed_time(e3) * 1e-3) / 1e12
     peaks = measured_peaks()
     peak = peaks.get("bf16_tflops")
     return {"bound": "tensor", "achieved": train_tf, "peak": peak, "unit": "TFLOP/s",
             "frac": train_tf / peak if peak else None, "traffic": None,
             "kernel": "gemm_kernel (tcgen05.mma kind::f16, bf16 in, fp32 TMEM accumulate)",
             "peak_source": f"bf16_tflops of {peaks['source']} (burst cuBLAS GEMM)",
-            "train_step_ms": e0.elapsed_time(e1) / steps, "train_batch": batch,
-            "inference_tflops": infer_tf, "inference_ms": e1.elapsed_time(e2), "inference_batch": infer_batch,
-            # input kernel + (L + 1) GEMMs forward; loss kernel + 2 (L + 1) GEMMs backward; Adam
-            "gpu_launches_per_train_step": 3 * n_layers + 5}
+            "train_step_ms": train_ms, "train_step": "one CUDA-graph replay (what MLP.train runs)",
+            "train_step_ms_eager": e0.elapsed_time(e1) / steps, "train_batch": batch,
+            "inference_tflops": infer_tf, "inference_ms": e2.elapsed_time(e3), "inference_batch": infer_batch,
+            # input kernel + (L + 1) GEMMs forward; loss kernel + 2 (L + 1) GEMMs backward; Adam + step count
+            "gpu_launches_per_train_step": 3 * n_layers + 6}
 
 
 def dictionary_model():

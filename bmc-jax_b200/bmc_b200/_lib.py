@@ -26,7 +26,8 @@ TANGENTS_AUTO, TANGENTS_FORWARD = 0, 1
 EXPORTS = ("bmc_abi_version", "bmc_version", "bmc_last_error", "bmc_release", "bmc_simulate",
            "bmc_simulate_jvp", "bmc_simulate_trajectory", "bmc_lm_fit", "bmc_normal_blocks",
            "bmc_simulate_counted", "bmc_simulate_jvp_counted", "bmc_probe_fma_peak", "bmc_simulate_noalloc",
-           "bmc_mlp_sizes", "bmc_mlp_sync", "bmc_mlp_forward", "bmc_mlp_backward", "bmc_mlp_adam_step", "bmc_uneven_create", "bmc_uneven_simulate",
+           "bmc_mlp_sizes", "bmc_mlp_sync", "bmc_mlp_forward", "bmc_mlp_backward", "bmc_mlp_adam_step",
+           "bmc_mlp_adam_step_dev", "bmc_uneven_create", "bmc_uneven_simulate",
            "bmc_uneven_destroy", "bmc_uneven_set_dense_switch", "bmc_normal_segments", "bmc_schur_step", "bmc_schur_eliminate", "bmc_schur_back",
            "bmc_set_tangent_mode")
 
@@ -131,7 +132,10 @@ def lib():
         L.bmc_mlp_backward.argtypes = [sp, vp, vp, C.c_int64, vp, vp, vp, vp]
         L.bmc_mlp_adam_step.argtypes = [sp, vp, vp, vp, vp, vp, C.c_int32, C.c_float, C.c_float, C.c_float,
                                         C.c_float, vp]
-        for f in ("bmc_mlp_sizes", "bmc_mlp_sync", "bmc_mlp_forward", "bmc_mlp_backward", "bmc_mlp_adam_step"):
+        L.bmc_mlp_adam_step_dev.argtypes = [sp, vp, vp, vp, vp, vp, vp, C.c_float, C.c_float, C.c_float, C.c_float,
+                                            vp]
+        for f in ("bmc_mlp_sizes", "bmc_mlp_sync", "bmc_mlp_forward", "bmc_mlp_backward", "bmc_mlp_adam_step",
+                  "bmc_mlp_adam_step_dev"):
             getattr(L, f).restype = C.c_int
         _lib = L
     return _lib

@@ -139,9 +139,18 @@ class MLP:
                                                 _lib.ptr(self.m), _lib.ptr(self.v), _lib.ptr(self.shadow),
                                                 self.step, lr, beta1, beta2, eps, _lib.stream_handle()))
 
-    def train(self, X, T, epochs: int = 10, batch: int = 4096, lr: float = 1e-3, seed: int = 0) -> List[float]:
+    def adam_dev(self, d_step, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8):
+        """Adam step with the step count in the device int32 `d_step` (advanced by the library)."""
+        _lib.check(_lib.lib().bmc_mlp_adam_step_dev(C.byref(self.shape), _lib.ptr(self.params), _lib.ptr(self.grad),
+                                                    _lib.ptr(self.m), _lib.ptr(self.v), _lib.ptr(self.shadow),
+                                                    _lib.ptr(d_step), lr, beta1, beta2, eps, _lib.stream_handle()))
+
+    def train(self, X, T, epochs: int = 10, batch: int = 4096, lr: float = 1e-3, seed: int = 0,
+              graph: bool = True) -> List[float]:
         """Adam on mean squared error over (X, T) (device float32 tensors); returns the mean training
-        loss of each epoch. The last partial batch of an epoch is dropped."""
+        loss of each epoch. The last partial batch of an epoch is dropped. With `graph`, one training step
+        (batch gather, forward, backward, Adam) is captured into a CUDA graph after the first step runs
+        eagerly, and replayed for the others; the step count lives on the device for that."""
         torch = _lib.torch_cuda()
         n = int(X.shape[0])
         if n < batch:
@@ -149,18 +158,36 @@ class MLP:
         g = torch.Generator(device="cuda")
         g.manual_seed(int(seed))
         loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+        d_step = torch.tensor([self.step], dtype=torch.int32, device="cuda")
+        idx = torch.empty(batch, dtype=torch.int64, device="cuda")
+
+        def one_step():
+            xb, tb = X.index_select(0, idx), T.index_select(0, idx)
+            self.forward(xb, keep=True)
+            self.backward(tb, loss)
+            self.adam_dev(d_step, lr)
+
         hist = []
         steps = n // batch
-        for _ in range(int(epochs)):
-            perm = torch.randperm(n, device="cuda", generator=g)
-            loss.zero_()
-            for s in range(steps):
-                idx = perm[s * batch:(s + 1) * batch]
-                xb, tb = X.index_select(0, idx), T.index_select(0, idx)
-                self.forward(xb, keep=True)
-                self.backward(tb, loss)
-                self.adam(lr)
-            hist.append(float(loss.item()) / steps)
+        captured = None
+        try:
+            for _ in range(int(epochs)):
+                perm = torch.randperm(n, device="cuda", generator=g)
+                loss.zero_()
+                for s in range(steps):
+                    idx.copy_(perm[s * batch:(s + 1) * batch])
+                    if captured is not None:
+                        captured.replay()
+                        continue
+                    one_step()
+                    if graph:
+                        captured = torch.cuda.CUDAGraph()
+                        with torch.cuda.graph(captured):
+                            one_step()
+                hist.append(float(loss.item()) / steps)
+        finally:
+            del captured
+        self.step = int(d_step.item())
         if self.status(batch) != 0:
             raise RuntimeError("a tensor-core GEMM gave up waiting during training (status word set)")
         return hist
@@ -208,20 +235,30 @@ class LadderWarmStart:
 
     # -- the simulator as the data source ------------------------------------------------------
     def simulate(self, X_phys, chunk: int = 131072):
-        """Z (float32, device) [n][n_points] of the Experiment with the free parameters set to X_phys."""
+        """Z (float32, device) [n][n_points] of the Experiment with the free parameters set to X_phys. The
+        spectra stay on the device: each chunk's float64 Z is rounded into the output there."""
         from .fitting import write_params
-        from .simulation import simulate_z, tile_params
+        from .simulation import (DeviceEvents, _device, n_cest_of, pack_params, problem, simulate_device,
+                                 state_size, tile_params)
         torch = _lib.torch_cuda()
         X_phys = np.asarray(X_phys, np.float64)
         n = X_phys.shape[0]
         out = torch.empty((n, self.n_points), dtype=torch.float32, device="cuda")
         ex = self.experiment
+        dev_ev = DeviceEvents(ex.events)
+        nc = n_cest_of(ex.params)
+        m0 = np.asarray(ex.m0, np.float64).reshape(-1, state_size(nc))
+        z = None
         for a in range(0, n, chunk):
             b = min(a + chunk, n)
-            base = tile_params(ex.params, b - a)
-            p = write_params(base, self.spec.to_scaled(X_phys[a:b]), self.spec)
-            z = simulate_z(p, ex.events, ex.m0, ex.mz_loc)
-            out[a:b] = torch.as_tensor(np.asarray(z, np.float32)).to("cuda")
+            p = write_params(tile_params(ex.params, b - a), self.spec.to_scaled(X_phys[a:b]), self.spec)
+            pdev = _device(pack_params(p, b - a))
+            mdev = _device(np.broadcast_to(m0, (b - a, m0.shape[1])))
+            if z is None or z.shape[0] != b - a:
+                z = torch.empty((b - a, dev_ev.n_offsets), dtype=torch.float64, device="cuda")
+            simulate_device(problem(b - a, dev_ev.n_offsets, dev_ev.n_events, nc, int(ex.mz_loc)), pdev, dev_ev,
+                            mdev, z)
+            out[a:b] = z.float()
         return out
 
     def simulate64(self, X_phys, chunk: int = 131072) -> np.ndarray:

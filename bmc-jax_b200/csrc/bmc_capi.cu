@@ -23,6 +23,7 @@
 #include "bmc_lm.cuh"
 #include "bmc_joint.cuh"
 #include "bmc_adjoint.cuh"
+#include "bmc_adjoint_block.cuh"
 
 using namespace bmc;
 
@@ -321,6 +322,25 @@ bmc_status launch_adjoint(const ChainArgs& a, const int* row_ev, int n_tan, cons
     return BMC_OK;
 }
 
+template <int NC>
+bmc_status launch_adjoint_block(const ChainArgs& a, const int4* blk, int n_tan, const TaylorTable* tt, cudaStream_t st) {
+    const size_t smem = kAdjBlkWarps * DenseGroup<NC>::G * sizeof(AdjBlkSlot<NC>);
+    static std::atomic<unsigned long long> configured{0};
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev >= 64 || !((configured.load(std::memory_order_acquire) >> dev) & 1ull)) {
+        CUDA_TRY(cudaFuncSetAttribute(adjoint_block_kernel<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+        if (dev < 64) configured.fetch_or(1ull << dev, std::memory_order_acq_rel);
+    }
+    const long long blocks = (a.n_chains + kAdjBlkWarps * 32 - 1) / (kAdjBlkWarps * 32);
+    if (blocks > 0x7fffffffLL) return fail(BMC_ERR_INVALID, "%lld chains exceed one launch", a.n_chains);
+    if (blocks == 0) return BMC_OK;
+    adjoint_block_kernel<NC><<<(unsigned)blocks, kAdjBlkWarps * 32, smem, st>>>(a, blk, n_tan, tt);
+    CUDA_TRY(cudaGetLastError());
+    return BMC_OK;
+}
+
 // Whether the tangents of a uniform table go through the adjoint kernel: two or more tangents, the
 // automatic mode, and every row a single-event row (adjoint_rows_kernel, which also fills row_ev). The
 // check reads one flag back, so a stream being captured keeps forward mode.
@@ -402,6 +422,8 @@ struct UnevenPlan {
     int4* seg = nullptr;       // the repeated block of every row of every table
     int* tab_row0 = nullptr;   // first row of each table in seg
     double dense_switch = 0.0; // > 0: the dense path's norm threshold for this plan (bmc_uneven_set_dense_switch)
+    int4* adj_blk = nullptr;   // per row: the block the adjoint block kernel takes (adjoint_block_rows_kernel)
+    int adj_ok = 0;            // every row of every table qualifies: tangents go through that kernel
     void* scratch = nullptr;   // sort keys and indices, cub scratch, status word
     size_t scratch_bytes = 0;
 };
@@ -448,6 +470,8 @@ struct Impl {
         for (int t = 0; t < tg->n_tangents; ++t) a.field_row[t] = tg->field_row[t];
         a.seed = tg->d_seed;
         a.dm0 = tg->d_dm0;
+        if (pl.adj_ok && tg->n_tangents >= 2 && g_tangent_mode.load(std::memory_order_relaxed) == BMC_TANGENTS_AUTO)
+            return launch_adjoint_block<NC>(a, pl.adj_blk, tg->n_tangents, tt, st);
         return run_tangents<NC, true>(a, tg->n_tangents, tt, st);
     }
 
@@ -876,6 +900,7 @@ bmc_status bmc_uneven_create(int32_t n_cest, int32_t n_voxels, const int32_t* h_
     if (e == cudaSuccess) e = cudaMalloc(&pl->scratch, pl->scratch_bytes);
     if (e == cudaSuccess) e = cudaMalloc(&pl->seg, sizeof(int4) * std::max<long long>(n_rows, 1));
     if (e == cudaSuccess) e = cudaMalloc(&pl->tab_row0, sizeof(int) * nt);
+    if (e == cudaSuccess) e = cudaMalloc(&pl->adj_blk, sizeof(int4) * std::max<long long>(n_rows, 1));
     if (e == cudaSuccess) e = cudaMemcpy(pl->tab_row0, row0.data(), sizeof(int) * nt, cudaMemcpyHostToDevice);
     if (e == cudaSuccess && nch) e = cudaMemcpy(pl->chain_map, cm.data(), sizeof(int2) * nch, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(pl->vox_table, h_voxel_table, sizeof(int) * n_voxels, cudaMemcpyHostToDevice);
@@ -900,9 +925,23 @@ bmc_status bmc_uneven_create(int32_t n_cest, int32_t n_voxels, const int32_t* h_
         else if (e == cudaSuccess)
             e = cudaMemset(pl->seg + row0[t], 0, sizeof(int4) * noff[t]);
     }
-    e = cudaGetLastError();
+    // the rows the adjoint block kernel takes (a flag in the plan's scratch, read back once here)
+    int* adj_flag = static_cast<int*>(pl->scratch);
+    if (e == cudaSuccess) e = cudaMemset(adj_flag, 1, sizeof(int));
+    for (int t = 0; t < nt && e == cudaSuccess; ++t) {
+        if (nev[t] > 0 && noff[t] > 0)
+            adjoint_block_rows_kernel<<<(noff[t] + 127) / 128, 128>>>(pl->rec + base[t], noff[t], nev[t], noff[t],
+                                                                     pl->seg + row0[t], reset_after_adc,
+                                                                     pl->adj_blk + row0[t], adj_flag);
+        else
+            e = cudaMemset(adj_flag, 0, sizeof(int));
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    int h_flag = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&h_flag, adj_flag, sizeof(int), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return undo(fail(BMC_ERR_CUDA, "uneven plan: %s", cudaGetErrorString(e)));
+    pl->adj_ok = h_flag != 0;
     if (n_chains) *n_chains = nch;
     if (h_chain_start) std::memcpy(h_chain_start, start.data(), sizeof(long long) * start.size());
     *plan = pl;
@@ -941,7 +980,7 @@ bmc_status bmc_uneven_destroy(void* plan) {
     UnevenPlan* pl = static_cast<UnevenPlan*>(plan);
     if (!pl) return BMC_OK;
     void* ptrs[] = {pl->rec, pl->chain_map, pl->vox_table, pl->tab_base, pl->tab_noff, pl->tab_nev, pl->scratch,
-                    pl->seg, pl->tab_row0};
+                    pl->seg, pl->tab_row0, pl->adj_blk};
     cudaError_t first = cudaSuccess;
     for (void* p : ptrs) {
         if (!p) continue;

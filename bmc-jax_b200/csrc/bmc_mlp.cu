@@ -26,6 +26,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -189,12 +190,14 @@ struct GemmArgs {
     int* status;
 };
 
+constexpr int kGemmStages = 3;   // K chunks in flight: a CTA's first three are all loaded before its first MMA
+
 template <int BN>
 struct GemmSmem {
     static constexpr uint32_t A_BYTES = 128 * 128;  // 128 rows x 64 bf16
     static constexpr uint32_t B_BYTES = BN * 128;
     static constexpr uint32_t STAGE = A_BYTES + B_BYTES;
-    static constexpr uint32_t BYTES = 2 * STAGE;
+    static constexpr uint32_t BYTES = kGemmStages * STAGE;
     static constexpr uint32_t NCOLS = BN < 32 ? 32 : BN;  // TMEM columns (power of two >= 32)
 };
 
@@ -280,17 +283,29 @@ __device__ __forceinline__ void epilogue(const GemmArgs& g, int row, int n, floa
     } else {  // EPI_DW
         if (live) {
             float* o = g.out + size_t(row) * g.ldo + n;
+            if ((reinterpret_cast<uintptr_t>(o) & 15) == 0) {
+                // one 16-byte reduction per four columns (global float4 atomics, sm_90 and later)
+                float4* o4 = reinterpret_cast<float4*>(o);
 #pragma unroll
-            for (int i = 0; i < 16; ++i) atomicAdd(o + i, v[i]);
+                for (int q = 0; q < 4; ++q)
+                    atomicAdd(o4 + q, make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]));
+            } else {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) atomicAdd(o + i, v[i]);
+            }
         }
     }
 }
 
+// 8 warps: the loads and the epilogue are spread over all of them (warps w and w + 4 read the same 32
+// TMEM lanes, w & 3, and take the two halves of the tile's columns); one thread issues the MMAs.
+constexpr int kGemmThreads = 256;
+
 template <int BN, int EPI>
-__global__ void __launch_bounds__(128, 1) gemm_kernel(GemmArgs g) {
+__global__ void __launch_bounds__(kGemmThreads, 2) gemm_kernel(GemmArgs g) {
     using S = GemmSmem<BN>;
     extern __shared__ __align__(1024) uint8_t smem[];
-    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ __align__(8) uint64_t bars[kGemmStages];
     __shared__ uint32_t tmem_slot;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -299,12 +314,11 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(GemmArgs g) {
     const int ke = min(g.K, kb + g.k_split);
     const int nk = (ke - kb) / 64;
     const uint32_t s0 = smem_addr(smem);
-    const uint32_t bar0 = smem_addr(&bars[0]), bar1 = smem_addr(&bars[1]);
 
     if (warp == 0) tmem_alloc(smem_addr(&tmem_slot), S::NCOLS);
     if (tid == 0) {
-        mbar_init(bar0, 1);
-        mbar_init(bar1, 1);
+#pragma unroll
+        for (int i = 0; i < kGemmStages; ++i) mbar_init(smem_addr(&bars[i]), 1);
         fence_barrier_init();
     }
     tc_fence_before();
@@ -314,50 +328,54 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(GemmArgs g) {
 
     auto load = [&](int stage, int k0) {
         const uint32_t a = s0 + stage * S::STAGE, b = a + S::A_BYTES;
-        for (int i = tid; i < 128 * 8; i += 128) {
+        for (int i = tid; i < 128 * 8; i += kGemmThreads) {
             const int r = i >> 3, c = i & 7;
             cp_async16(a + (r >> 3) * 1024 + c * 128 + (r & 7) * 16, g.A + size_t(m0 + r) * g.lda + k0 + c * 8);
         }
-        for (int i = tid; i < BN * 8; i += 128) {
+        for (int i = tid; i < BN * 8; i += kGemmThreads) {
             const int r = i >> 3, c = i & 7;
             cp_async16(b + (r >> 3) * 1024 + c * 128 + (r & 7) * 16, g.B + size_t(n0 + r) * g.ldb + k0 + c * 8);
         }
         cp_async_commit();
     };
 
+    // Chunk c uses stage c % kGemmStages; its MMAs are committed to that stage's barrier (phase c / stages),
+    // which the CTA waits for before the stage takes chunk c + stages.
     bool ok = true;
-    int committed = -1;  // last chunk whose MMAs were committed
-    if (nk > 0) load(0, kb);
+    int issued = 0;   // chunks whose loads were issued
+    for (; issued < min(nk, kGemmStages); ++issued) load(issued, kb + issued * 64);
+    int committed = -1;
     for (int c = 0; ok && c < nk; ++c) {
-        const int s = c & 1;
-        if (c + 1 < nk) {
-            // stage s^1 was read by the MMAs of chunk c-1: wait for them before overwriting it
-            bool w = true;
-            if (c >= 1) w = mbar_wait((s ^ 1) ? bar1 : bar0, ((c - 1) >> 1) & 1);
-            if (!__syncthreads_and(w)) {
-                ok = false;
-                break;
-            }
-            load(s ^ 1, kb + (c + 1) * 64);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
+        const int st = c % kGemmStages;
+        const int pending = issued - (c + 1);   // later chunks' load groups that may still be in flight
+        if (pending >= 2) cp_async_wait<2>();
+        else if (pending == 1) cp_async_wait<1>();
+        else cp_async_wait<0>();
         fence_proxy_async();  // this thread's cp.async writes -> visible to the tensor core
         __syncthreads();
         if (tid == 0) {
             tc_fence_after();
-            const uint32_t a = s0 + s * S::STAGE, b = a + S::A_BYTES;
+            const uint32_t a = s0 + st * S::STAGE, b = a + S::A_BYTES;
 #pragma unroll
             for (int j = 0; j < 4; ++j)
                 umma_bf16(tmem, smem_desc(a + j * 256), smem_desc(b + j * 256), idesc_bf16(BN), (c | j) != 0);
-            umma_commit(s ? bar1 : bar0);
+            umma_commit(smem_addr(&bars[st]));
         }
         committed = c;
+        if (issued < nk) {
+            // the stage is free once chunk c's MMAs are done
+            const bool w = mbar_wait(smem_addr(&bars[st]), (c / kGemmStages) & 1);
+            if (!__syncthreads_and(w)) {
+                ok = false;
+                break;
+            }
+            load(st, kb + issued * 64);
+            ++issued;
+        }
     }
     if (committed >= 0) {
         // the last commit covers every earlier MMA of the CTA
-        const bool w = mbar_wait((committed & 1) ? bar1 : bar0, (committed >> 1) & 1);
+        const bool w = mbar_wait(smem_addr(&bars[committed % kGemmStages]), (committed / kGemmStages) & 1);
         ok = ok && w;
     }
     ok = __syncthreads_and(ok);
@@ -365,10 +383,11 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(GemmArgs g) {
     tc_fence_after();
 
     if (ok && nk > 0) {
-        const int row = m0 + warp * 32 + lane;
-        const uint32_t trow = tmem + (uint32_t(warp * 32) << 16);
+        const int quarter = warp & 3, half = warp >> 2;
+        const int row = m0 + quarter * 32 + lane;
+        const uint32_t trow = tmem + (uint32_t(quarter * 32) << 16);
 #pragma unroll 1
-        for (int cb = 0; cb < BN; cb += 16) {
+        for (int cb = half * (BN / 2); cb < (half + 1) * (BN / 2); cb += 16) {
             float v[16];
             tmem_ld16(trow + cb, v);
             epilogue<EPI>(g, row, n0 + cb, v);
@@ -476,6 +495,29 @@ __global__ void adam_kernel(LayerMap L, float* __restrict__ p, const float* __re
         refresh_shadow(L, k, w, shadow);
     }
 }
+
+// Adam with the step count on the device (a CUDA graph replays it unchanged): the bias-corrected rate of
+// step *d_step + 1, computed by every thread as the host entry computes it; the count is advanced by
+// step_advance_kernel after the update.
+__global__ void adam_dev_kernel(LayerMap L, float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                                float* __restrict__ v, long long n, const int* __restrict__ d_step, float lr, float b1,
+                                float b2, float eps, bf16* __restrict__ shadow) {
+    const double t = double(*d_step + 1);
+    const float lr_t = float(double(lr) * sqrt(1.0 - pow(double(b2), t)) / (1.0 - pow(double(b1), t)));
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x) {
+        const float gk = g[k];
+        const float mk = b1 * m[k] + (1.0f - b1) * gk;
+        const float vk = b2 * v[k] + (1.0f - b2) * gk * gk;
+        m[k] = mk;
+        v[k] = vk;
+        const float w = p[k] - lr_t * mk / (sqrtf(vk) + eps);
+        p[k] = w;
+        refresh_shadow(L, k, w, shadow);
+    }
+}
+
+__global__ void step_advance_kernel(int* d_step) { *d_step += 1; }
 
 // ------------------------------------------------------------------------------------------------
 // host side: shapes, buffer carving, launches
@@ -586,15 +628,17 @@ Work carve(const Shape& s, long long batch, void* base) {
 template <int BN, int EPI>
 bmc_status launch_gemm_t(const GemmArgs& g, int splits, cudaStream_t st) {
     using S = GemmSmem<BN>;
-    static unsigned long long configured = 0;  // one bit per device, per instantiation
+    // the attribute once per device and instantiation (later calls only enqueue work, which keeps them
+    // capturable); atomic, as calls on several devices may come from several threads
+    static std::atomic<unsigned long long> configured{0};
     int dev = 0;
     MLP_CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 64 && !((configured >> dev) & 1ull)) {
+    if (dev >= 64 || !((configured.load(std::memory_order_acquire) >> dev) & 1ull)) {
         MLP_CUDA_TRY(cudaFuncSetAttribute(gemm_kernel<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::BYTES));
-        configured |= 1ull << dev;
+        if (dev < 64) configured.fetch_or(1ull << dev, std::memory_order_acq_rel);
     }
     dim3 grid(g.M / 128, g.N / BN, splits);
-    gemm_kernel<BN, EPI><<<grid, 128, S::BYTES, st>>>(g);
+    gemm_kernel<BN, EPI><<<grid, kGemmThreads, S::BYTES, st>>>(g);
     MLP_CUDA_TRY(cudaGetLastError());
     return BMC_OK;
 }
@@ -610,12 +654,15 @@ bmc_status gemm(GemmArgs g, int splits, cudaStream_t st) {
     splits = std::max(1, std::min(splits, chunks));
     g.k_split = int(rup(chunks, splits) / splits) * 64;
     splits = int((g.K + g.k_split - 1) / g.k_split);
-    if (g.N % 128 == 0) return launch_gemm_t<128, EPI>(g, splits, st);
+    // 128-wide tiles where they fill the SMs, else 64-wide (twice the CTAs)
+    if (g.N % 128 == 0 && (long long)(g.M / 128) * (g.N / 128) * splits >= 148) return launch_gemm_t<128, EPI>(g, splits, st);
     return launch_gemm_t<64, EPI>(g, splits, st);
 }
 
+// split-K of a weight gradient: about one CTA per SM over 64-wide tiles (what `gemm` takes for these
+// shapes), each CTA accumulating whole 64-deep chunks before its atomics
 int dw_splits(int M, int N, int K) {
-    const int tiles = (M / 128) * (N % 128 == 0 ? N / 128 : N / 64);
+    const int tiles = (M / 128) * (N / 64);
     return std::max(1, std::min(K / 64, 148 / std::max(1, tiles)));
 }
 
@@ -813,6 +860,24 @@ bmc_status bmc_mlp_adam_step(const bmc_mlp_shape* shape, float* d_params, const 
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
     adam_kernel<<<unsigned(std::min<long long>((n + 255) / 256, 4096)), 256, 0, st>>>(
         layer_map(s), d_params, d_grad, d_m, d_v, n, float(lr_t), beta1, beta2, eps, static_cast<bf16*>(d_shadow));
+    MLP_CUDA_TRY(cudaGetLastError());
+    return BMC_OK;
+}
+
+bmc_status bmc_mlp_adam_step_dev(const bmc_mlp_shape* shape, float* d_params, const float* d_grad, float* d_m,
+                                 float* d_v, void* d_shadow, int32_t* d_step, float lr, float beta1, float beta2,
+                                 float eps, void* stream) {
+    Shape s;
+    if (bmc_status e = check_shape(shape, &s)) return e;
+    if (!d_params || !d_grad || !d_m || !d_v || !d_shadow || !d_step) return fail(BMC_ERR_INVALID, "null Adam operand");
+    if (!(lr > 0) || !(beta1 >= 0 && beta1 < 1) || !(beta2 >= 0 && beta2 < 1) || !(eps > 0))
+        return fail(BMC_ERR_INVALID, "Adam: lr %g, beta1 %g, beta2 %g, eps %g", lr, beta1, beta2, eps);
+    const long long n = n_params(s);
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    adam_dev_kernel<<<unsigned(std::min<long long>((n + 255) / 256, 4096)), 256, 0, st>>>(
+        layer_map(s), d_params, d_grad, d_m, d_v, n, d_step, lr, beta1, beta2, eps, static_cast<bf16*>(d_shadow));
+    MLP_CUDA_TRY(cudaGetLastError());
+    step_advance_kernel<<<1, 1, 0, st>>>(d_step);
     MLP_CUDA_TRY(cudaGetLastError());
     return BMC_OK;
 }

@@ -332,6 +332,11 @@ bmc_status bmc_mlp_backward(const bmc_mlp_shape* shape, const void* d_shadow, co
 bmc_status bmc_mlp_adam_step(const bmc_mlp_shape* shape, float* d_params, const float* d_grad, float* d_m,
                              float* d_v, void* d_shadow, int32_t step, float lr, float beta1, float beta2, float eps,
                              void* stream);
+/* bmc_mlp_adam_step with the step count on the device: step *d_step + 1, then *d_step is advanced, so
+ * that a training step captured into a CUDA graph can be replayed. */
+bmc_status bmc_mlp_adam_step_dev(const bmc_mlp_shape* shape, float* d_params, const float* d_grad, float* d_m,
+                                 float* d_v, void* d_shadow, int32_t* d_step, float lr, float beta1, float beta2,
+                                 float eps, void* stream);
 
 /*
  * Diagnostics (no counterpart in the reference: measurement support for the benchmark).

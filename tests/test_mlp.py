@@ -183,6 +183,40 @@ def test_adam_step_and_shadow_match_the_oracle(cuda):
 
 
 @pytest.mark.gpu
+def test_adam_with_the_step_on_the_device(cuda):
+    """bmc_mlp_adam_step_dev: the same update as the host-step entry, and the count advanced."""
+    torch = cuda
+    a, b = _net(SMALL, seed=4), _net(SMALL, seed=4)
+    rng = np.random.default_rng(9)
+    g = torch.as_tensor(rng.normal(0, 1e-2, a.params.numel()).astype(np.float32)).cuda() * (a.params != 0)
+    for net in (a, b):
+        net.grad.copy_(g)
+    a.step = 6
+    a.adam(lr=1e-3)
+    d_step = torch.tensor([6], dtype=torch.int32, device="cuda")
+    b.adam_dev(d_step, lr=1e-3)
+    assert int(d_step.item()) == 7
+    np.testing.assert_allclose(b.params.cpu().numpy(), a.params.cpu().numpy(), rtol=1e-6, atol=1e-9)
+    np.testing.assert_allclose(b.m.cpu().numpy(), a.m.cpu().numpy(), rtol=0, atol=0)
+
+
+@pytest.mark.gpu
+def test_graph_replayed_training_follows_the_eager_loop(cuda):
+    """Training with the captured step takes the eager loop's steps (float atomics reorder sums: close,
+    not equal)."""
+    torch = cuda
+    rng = np.random.default_rng(21)
+    x = torch.as_tensor(rng.normal(0, 1, (8192, SMALL[0])).astype(np.float32)).cuda()
+    t = torch.as_tensor(rng.normal(0, 0.5, (8192, SMALL[3])).astype(np.float32)).cuda()
+    a, b = _net(SMALL, seed=5), _net(SMALL, seed=5)
+    ha = a.train(x, t, epochs=3, batch=1024, lr=1e-3, seed=2, graph=True)
+    hb = b.train(x, t, epochs=3, batch=1024, lr=1e-3, seed=2, graph=False)
+    assert a.step == b.step == 24
+    np.testing.assert_allclose(ha, hb, rtol=1e-3)
+    np.testing.assert_allclose(a.params.cpu().numpy(), b.params.cpu().numpy(), rtol=1e-2, atol=1e-4)
+
+
+@pytest.mark.gpu
 def test_training_fits_a_teacher_network(cuda):
     """A student learns a random teacher's function: the loss falls by more than 10x."""
     torch = cuda
