@@ -188,3 +188,67 @@ def test_pulse_trains_stay_in_forward_mode(cuda):
     np.testing.assert_array_equal(za, zf)
     np.testing.assert_array_equal(ja, jf)
     np.testing.assert_array_equal(wa, wf)
+
+
+# ------------------------------------------------------------------------------------------------
+# uneven batches: the block kernel (rows = a block of pulse and gap repeated r times, then the readout)
+# ------------------------------------------------------------------------------------------------
+def _block_table(ppm, b1s, n_pulses, tp=0.05, gap=0.005, b0=3.0):
+    from bmc_b200.simulation import SimEvent
+    rows = [(b, p) for b in b1s for p in ppm]
+    n, ne = len(rows), 2 * n_pulses + 1
+    return SimEvent(np.tile(np.int32([1, 0] * n_pulses + [3]), (n, 1)),
+                    np.tile([tp, gap] * n_pulses + [0.0], (n, 1)),
+                    np.array([[b * 267.5153 / (2 * np.pi), 0.0] * n_pulses + [0.0] for b, _ in rows]),
+                    np.zeros((n, ne)),
+                    np.array([[p * 42.5764 * b0, 0.0] * n_pulses + [0.0] for _, p in rows]),
+                    np.tile(np.int32([-1] * (ne - 1) + [0]), (n, 1)))
+
+
+def _uneven_tangents(g, slots, nc, seeds, dm0, mode):
+    import torch
+    from bmc_b200 import _lib, settings
+    from bmc_b200.fitting import field_row
+    P = len(slots)
+    tg = _lib.Tangents()
+    tg.n_tangents = P
+    for i, (f, ix) in enumerate(slots):
+        tg.field_row[i] = field_row(f, ix, nc)
+    tg.d_seed, tg.d_dm0 = seeds.data_ptr(), dm0.data_ptr()
+    settings.use_tangents(mode)
+    try:
+        jz = torch.empty((P, g.n_chains), dtype=torch.float64, device="cuda")
+        z = g.plan.run(g.params, g.m0, tg, jz)
+        torch.cuda.synchronize()
+        return z.cpu().numpy(), jz.cpu().numpy()
+    finally:
+        settings.use_tangents("auto")
+
+
+@pytest.mark.parametrize("nc,mt", [(1, False), (2, True), (4, False), (5, True)])
+def test_uneven_block_tangents_equal_forward_mode(cuda, nc, mt):
+    """Voxels of one pool count with trains of 1, 2, 7 and 40 block pulses (no block, and blocks of 2 to
+    40 repeats), seven tangents of every kind with per-voxel seeds and a start-state tangent: the block
+    kernel against forward mode (one chain-kernel launch per tangent)."""
+    import torch
+    from bmc_b200.fitting import Experiment
+    from bmc_b200.simulation import SimParams
+    from bmc_b200.uneven import UnevenBatch
+    rng = np.random.default_rng(50 + nc)
+    tables = [_block_table(np.linspace(-5, 5, 7), (0.8, 2.5), n) for n in (1, 2, 7, 40)]
+    pb = _batch(8, nc, seed=60 + nc, mt=mt)
+    exps = [Experiment(SimParams(*O.sample(pb, i)), tables[i % 4], O.initial_state(O.sample(pb, i)), O.mz_loc(nc))
+            for i in range(8)]
+    g = UnevenBatch(exps).groups[0]
+    slots = [("cest_k", 0), ("cest_f", nc - 1), ("water_r2", None), ("water_r1", None), ("b0_inhom", None),
+             ("rel_b1", None), ("mt_k" if mt else "cest_r2", None if mt else 0)]
+    P, nv, N = len(slots), len(g.voxels), 3 * nc + 4
+    seeds = torch.as_tensor(rng.normal(size=(P, nv))).cuda()
+    dm0 = torch.zeros((P, nv, N), dtype=torch.float64, device="cuda")
+    dm0[2] = torch.as_tensor(rng.normal(size=(nv, N)) * 0.1)
+    za, ja = _uneven_tangents(g, slots, nc, seeds, dm0, "auto")
+    zf, jf = _uneven_tangents(g, slots, nc, seeds, dm0, "forward")
+    np.testing.assert_allclose(za, zf, rtol=0, atol=1e-12)
+    for p in range(P):
+        np.testing.assert_allclose(ja[p], jf[p], rtol=1e-8, atol=1e-10 * max(1.0, np.abs(jf[p]).max()),
+                                   err_msg=f"tangent {slots[p]}")
