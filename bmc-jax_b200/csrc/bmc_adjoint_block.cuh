@@ -230,12 +230,14 @@ struct AdjBlk {
             }
             __syncwarp();
             if (sq) {
+                // the lane's own column is read back from shared memory, so that the l loop need not index
+                // registers and can stay partly rolled
                 S nv;
 #pragma unroll
                 for (int r = 0; r < N; ++r) C0::at(nv, r).v = caug * T[N * LD + r];
-#pragma unroll
+#pragma unroll 4
                 for (int l = 0; l < N; ++l) {
-                    const double w = C0::at(cv, l).v;
+                    const double w = T[gl * LD + l];
 #pragma unroll
                     for (int r = 0; r < N; ++r) C0::at(nv, r).v = fma(T[l * LD + r], w, C0::at(nv, r).v);
                 }
@@ -262,30 +264,37 @@ struct AdjBlk {
         if (work) {
             const double e2 = sl->scale[i];
             const double* W = sl->B;
+            // this lane's current column, stored where the squarings' T will go (free until then): the
+            // dense product with W_i reads its multipliers back from there, so that its l loop stays rolled
+            // (fully unrolled, that product's 17 x 17 loads spilled registers)
+            double* col = sl->P + gl * LD;
             for (int k = tt.dense_m; k >= 1; --k) {
-                S yv, yd;
-                op(sl, i, cv, caug, yv);
-                op(sl, i, cd, cdN, yd);
-                // (W_i / 2^s) [cv; caug]
-                double wn = 0.0;
-                S wv;
-#pragma unroll
-                for (int q = 0; q < N; ++q) C0::at(wv, q).v = W[N * LD + q] * caug;
-                wn = W[N * LD + N] * caug;
-#pragma unroll
-                for (int l = 0; l < N; ++l) {
-                    const double x = C0::at(cv, l).v;
-#pragma unroll
-                    for (int q = 0; q < N; ++q) C0::at(wv, q).v = fma(W[l * LD + q], x, C0::at(wv, q).v);
-                    wn = fma(W[l * LD + N], x, wn);
-                }
                 const double ik = tt.inv_k[k];
 #pragma unroll
-                for (int q = 0; q < N; ++q) {
-                    C0::at(cv, q).v = (q == gl ? 1.0 : 0.0) + ik * C0::at(yv, q).v;
-                    C0::at(cd, q).v = ik * fma(e2, C0::at(wv, q).v, C0::at(yd, q).v);
+                for (int q = 0; q < N; ++q) col[q] = C0::at(cv, q).v;
+                // tangent column first, from the current cv: cd <- (X_s cd + (W_i / 2^s) [cv; caug]) / k
+                {
+                    S yd;
+                    op(sl, i, cd, cdN, yd);
+                    double wn = e2 * W[N * LD + N] * caug;
+#pragma unroll
+                    for (int q = 0; q < N; ++q) C0::at(yd, q).v = fma(e2 * W[N * LD + q], caug, C0::at(yd, q).v);
+#pragma unroll 2
+                    for (int l = 0; l < N; ++l) {
+                        const double x = e2 * col[l];
+#pragma unroll
+                        for (int q = 0; q < N; ++q) C0::at(yd, q).v = fma(W[l * LD + q], x, C0::at(yd, q).v);
+                        wn = fma(W[l * LD + N], x, wn);
+                    }
+#pragma unroll
+                    for (int q = 0; q < N; ++q) C0::at(cd, q).v = ik * C0::at(yd, q).v;
+                    cdN = ik * wn;
                 }
-                cdN = ik * e2 * wn;
+                // then the primal column: cv <- e_gl + X_s [cv; caug] / k
+                S yv;
+                op(sl, i, cv, caug, yv);
+#pragma unroll
+                for (int q = 0; q < N; ++q) C0::at(cv, q).v = (q == gl ? 1.0 : 0.0) + ik * C0::at(yv, q).v;
             }
         }
         __syncwarp();   // W_i is read by every lane before the squarings overwrite B
@@ -312,9 +321,9 @@ struct AdjBlk {
                     C0::at(nd, r).v = fma(t_aug, cdN, caug * h_aug);
                 }
                 ndN = fma(caug, H[N * LD + N], ndN);
-#pragma unroll
+#pragma unroll 2
                 for (int l = 0; l < N; ++l) {
-                    const double wv = C0::at(cv, l).v, wd = C0::at(cd, l).v;
+                    const double wv = T[gl * LD + l], wd = H[gl * LD + l];   // this lane's column, as stored
 #pragma unroll
                     for (int r = 0; r < N; ++r) {
                         const double t = T[l * LD + r];
