@@ -10,6 +10,7 @@
 #include <type_traits>
 
 #include "bmc_device.cuh"
+#include "bmc_tail32.cuh"
 
 namespace bmc {
 
@@ -382,21 +383,21 @@ struct Chain {
                 }
                 if constexpr (kMixed) {
                     if (k <= m_w) {
-                        using C32 = Chain<NC, float, 0>;
-                        using F = Dn<float, 0>;
-                        StepCoef<NC, F> s32;
-                        State<NC, F> t32, a32;
-                        to_float(s, s32);
-                        to_float(term, t32);
-                        zero_state(a32);
+                        // paired float32 instructions over the CEST pools (bmc_tail32.cuh)
+                        using T32 = Tail32<NC>;
+                        typename T32::Coef s32;
+                        typename T32::St t32, a32;
+                        T32::coef(s, s32);
+                        T32::state(term, t32);
+                        T32::zero(a32);
 #pragma unroll 1
                         for (; k <= m_w; ++k) {
-                            State<NC, F> n32;
-                            C32::template matvec<false>(s32, t32, n32);
+                            typename T32::St n32;
+                            T32::matvec(s32, t32, n32);
                             t32 = n32;
-                            C32::fma_state(a32, k <= m_on ? tt.inv_fact_f[k] : 0.f, t32);
+                            T32::fma_acc(a32, k <= m_on ? tt.inv_fact_f[k] : 0.f, t32);
                         }
-                        add_float(M, a32);
+                        T32::add_to(M, a32);
                     }
                 }
             } while (pend);
