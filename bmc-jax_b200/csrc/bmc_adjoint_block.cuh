@@ -341,7 +341,8 @@ struct AdjBlk {
     }
 };
 
-template <int NC>
+// kTan false: z only (phases A, B and D without W), for the plan's primal passes
+template <int NC, bool kTan>
 __global__ void __launch_bounds__(32 * kAdjBlkWarps, 2)
 adjoint_block_kernel(const ChainArgs a, const int4* __restrict__ blk, int n_tan, const TaylorTable* __restrict__ ttab) {
     using AB = AdjBlk<NC>;
@@ -405,7 +406,11 @@ adjoint_block_kernel(const ChainArgs a, const int4* __restrict__ blk, int n_tan,
                     int s = 0;
                     Dn<double, 3> g3 = dconst<double, 3>(0.0);
                     if (moves) {
-                        if (cc.mt_on && cc.ls != 0 && rec.w1 != 0.0) {
+                        if (!kTan && cc.mt_on && cc.ls != 0 && rec.w1 != 0.0) {
+                            const D0 offmt = (rec.wf - cc.dw0) - cc.dwmt;
+                            g3.v = (cc.ls == 1 ? lorentzian<double, 0>(offmt, cc.t2mt)
+                                               : super_lorentzian<double, 0>(offmt, cc.t2mt, cc.w0sl)).v;
+                        } else if (kTan && cc.mt_on && cc.ls != 0 && rec.w1 != 0.0) {
                             Dn<double, 3> off3 = dconst<double, 3>(((rec.wf - cc.dw0) - cc.dwmt).v);
                             Dn<double, 3> t23 = dconst<double, 3>(cc.t2mt.v), w03 = dconst<double, 3>(cc.w0sl.v);
                             off3.d[0] = 1.0;
@@ -433,8 +438,9 @@ adjoint_block_kernel(const ChainArgs a, const int4* __restrict__ blk, int n_tan,
                         sl->h[i] = h;
                         sl->scale[i] = ldexp(1.0, -s);
                         if (a.work) {
-                            wk1 += unsigned(2 * NA * tt.dense_m);   // exponential and Frechet derivative
-                            wk2 += unsigned(2 * s);
+                            // the exponential (and with tangents its Frechet derivative)
+                            wk1 += unsigned((kTan ? 2 : 1) * NA * tt.dense_m);
+                            wk2 += unsigned((kTan ? 2 : 1) * s);
                         }
                     }
                     sl->s[i] = s;
@@ -452,8 +458,10 @@ adjoint_block_kernel(const ChainArgs a, const int4* __restrict__ blk, int n_tan,
             const int Lmax = (int)__reduce_max_sync(kFull, (unsigned)L);
             const int rmax = (int)__reduce_max_sync(kFull, (unsigned)r);
             // tangent coefficient sets: lane task q = (event, tangent)
-            if (have)
-                for (int q = gl; q < L * n_tan; q += GS) AB::tangent_set(a, sl, node, q / n_tan, q % n_tan);
+            if constexpr (kTan) {
+                if (have)
+                    for (int q = gl; q < L * n_tan; q += GS) AB::tangent_set(a, sl, node, q / n_tan, q % n_tan);
+            }
             // A: the events' propagators
             for (int i = 0; i < Lmax; ++i) {
                 const bool mv = have && i < L && sl->moves[i];
@@ -471,24 +479,27 @@ adjoint_block_kernel(const ChainArgs a, const int4* __restrict__ blk, int n_tan,
                     if (sl->moves[i]) AB::mat_vec(sl->E[i], x);
             if (work) AB::store_col(sl->P, gl, x);
             __syncwarp();
-            // C: adjoint states b_{m+1} = P^T b_m from b_0 = lam, b_m in vec[m & 1]; lane gl keeps its entries
-            // (x = P[:, gl])
-            if (work) sl->vec[0][gl] = gl == a.mz ? 1.0 : 0.0;
-            __syncwarp();
-            for (int m = 0; m < rmax; ++m) {
-                double bn = 0.0;
-                if (work && m < r) {
-                    const double* bv = sl->vec[m & 1];
-                    bh[m] = bv[gl];
-#pragma unroll
-                    for (int l = 0; l < NA; ++l) bn = fma(x[l], bv[l], bn);
-                }
+            double b_r = 0.0;
+            if constexpr (kTan) {
+                // C: adjoint states b_{m+1} = P^T b_m from b_0 = lam, b_m in vec[m & 1]; lane gl keeps its entries
+                // (x = P[:, gl])
+                if (work) sl->vec[0][gl] = gl == a.mz ? 1.0 : 0.0;
                 __syncwarp();
-                if (work && m < r) sl->vec[(m + 1) & 1][gl] = bn;
+                for (int m = 0; m < rmax; ++m) {
+                    double bn = 0.0;
+                    if (work && m < r) {
+                        const double* bv = sl->vec[m & 1];
+                        bh[m] = bv[gl];
+#pragma unroll
+                        for (int l = 0; l < NA; ++l) bn = fma(x[l], bv[l], bn);
+                    }
+                    __syncwarp();
+                    if (work && m < r) sl->vec[(m + 1) & 1][gl] = bn;
+                    __syncwarp();
+                }
+                b_r = work ? sl->vec[r & 1][gl] : 0.0;
                 __syncwarp();
             }
-            const double b_r = work ? sl->vec[r & 1][gl] : 0.0;
-            __syncwarp();
             // D: forward states a_{k+1} = P a_k from a_0 = [M0; 1], a_k in vec[k & 1]; lane gl accumulates
             // column gl of W
             if (work) {
@@ -503,9 +514,11 @@ adjoint_block_kernel(const ChainArgs a, const int4* __restrict__ blk, int n_tan,
                 double an = 0.0;
                 if (work && k < r) {
                     const double* av = sl->vec[k & 1];
-                    const double bj = bh[r - 1 - k];
+                    if constexpr (kTan) {
+                        const double bj = bh[r - 1 - k];
 #pragma unroll
-                    for (int q = 0; q < NA; ++q) w[q] = fma(av[q], bj, w[q]);
+                        for (int q = 0; q < NA; ++q) w[q] = fma(av[q], bj, w[q]);
+                    }
 #pragma unroll
                     for (int l = 0; l < NA; ++l) an = fma(sl->P[l * LD + gl], av[l], an);
                 }
@@ -514,56 +527,58 @@ adjoint_block_kernel(const ChainArgs a, const int4* __restrict__ blk, int n_tan,
                 __syncwarp();
             }
             const double z = have ? sl->vec[r & 1][a.mz] : 0.0;
-            if (work) AB::store_col(sl->A, gl, w);
-            __syncwarp();
-            // E: per event, from the last: W_i = (E_{i-1} ... E_0) R_i with R_i = W E_{L-1} ... E_{i+1} (in A),
-            // then G_i = L(X_i, W_i) and the contractions
             double gacc[kMaxT];
 #pragma unroll
             for (int p = 0; p < kMaxT; ++p) gacc[p] = 0.0;
-            for (int i = Lmax - 1; i >= 0; --i) {
-                const bool mv = have && i < L && sl->moves[i];
-                if (work && mv) {
-                    AB::load_col(sl->A, gl, x);
-                    for (int q = 0; q < i; ++q)
-                        if (sl->moves[q]) AB::mat_vec(sl->E[q], x);
-                    AB::store_col(sl->B, gl, x);
-                }
+            if constexpr (kTan) {
+                if (work) AB::store_col(sl->A, gl, w);
                 __syncwarp();
-                const int s_g = mv ? sl->s[i] : 0;
-                const int smax = (int)__reduce_max_sync(kFull, (unsigned)s_g);
-                S cd;
-                double cdN;
-                AB::frechet_event(sl, i, gl, work && mv, s_g, smax, tt, cd, cdN);
-                if (work && mv && gl < N) {
-#pragma unroll
-                    for (int p = 0; p < kMaxT; ++p)
-                        if (p < n_tan) gacc[p] += AB::dop_row(sl, i, p, cd, cdN, gl);
-                }
-                // R_{i-1} = R_i E_i: column gl is R_i E_i[:, gl]
-                if (i > 0) {
-                    double y[NA];
+                // E: per event, from the last: W_i = (E_{i-1} ... E_0) R_i with R_i = W E_{L-1} ... E_{i+1} (in A),
+                // then G_i = L(X_i, W_i) and the contractions
+                for (int i = Lmax - 1; i >= 0; --i) {
+                    const bool mv = have && i < L && sl->moves[i];
                     if (work && mv) {
-#pragma unroll
-                        for (int q = 0; q < NA; ++q) y[q] = 0.0;
-                        const double* Ei = sl->E[i];
-#pragma unroll
-                        for (int l = 0; l < NA; ++l) {
-                            const double e = Ei[gl * LD + l];
-#pragma unroll
-                            for (int q = 0; q < NA; ++q) y[q] = fma(sl->A[l * LD + q], e, y[q]);
-                        }
+                        AB::load_col(sl->A, gl, x);
+                        for (int q = 0; q < i; ++q)
+                            if (sl->moves[q]) AB::mat_vec(sl->E[q], x);
+                        AB::store_col(sl->B, gl, x);
                     }
                     __syncwarp();
-                    if (work && mv) AB::store_col(sl->A, gl, y);
-                    __syncwarp();
-                }
-            }
-            // the start state's tangents: (P^r)^T lam . dv_p
-            if (work && gl < N && a.dm0) {
+                    const int s_g = mv ? sl->s[i] : 0;
+                    const int smax = (int)__reduce_max_sync(kFull, (unsigned)s_g);
+                    S cd;
+                    double cdN;
+                    AB::frechet_event(sl, i, gl, work && mv, s_g, smax, tt, cd, cdN);
+                    if (work && mv && gl < N) {
 #pragma unroll
-                for (int p = 0; p < kMaxT; ++p)
-                    if (p < n_tan) gacc[p] = fma(b_r, a.dm0[((size_t)p * a.n_vox + sl->vox) * N + gl], gacc[p]);
+                        for (int p = 0; p < kMaxT; ++p)
+                            if (p < n_tan) gacc[p] += AB::dop_row(sl, i, p, cd, cdN, gl);
+                    }
+                    // R_{i-1} = R_i E_i: column gl is R_i E_i[:, gl]
+                    if (i > 0) {
+                        double y[NA];
+                        if (work && mv) {
+#pragma unroll
+                            for (int q = 0; q < NA; ++q) y[q] = 0.0;
+                            const double* Ei = sl->E[i];
+#pragma unroll
+                            for (int l = 0; l < NA; ++l) {
+                                const double e = Ei[gl * LD + l];
+#pragma unroll
+                                for (int q = 0; q < NA; ++q) y[q] = fma(sl->A[l * LD + q], e, y[q]);
+                            }
+                        }
+                        __syncwarp();
+                        if (work && mv) AB::store_col(sl->A, gl, y);
+                        __syncwarp();
+                    }
+                }
+                // the start state's tangents: (P^r)^T lam . dv_p
+                if (work && gl < N && a.dm0) {
+#pragma unroll
+                    for (int p = 0; p < kMaxT; ++p)
+                        if (p < n_tan) gacc[p] = fma(b_r, a.dm0[((size_t)p * a.n_vox + sl->vox) * N + gl], gacc[p]);
+                }
             }
 #pragma unroll
             for (int p = 0; p < kMaxT; ++p) {

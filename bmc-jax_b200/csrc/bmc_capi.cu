@@ -235,7 +235,8 @@ bmc_status fill_spread(ChainArgs& a, const bmc_spread* sp) {
 // the repeated block of every row of a table of records (block_scan_kernel), into seg[n_rows]
 bmc_status scan_blocks(const EvRec<double>* rec, int n_rows, int n_ev, int stride, int4* seg, cudaStream_t st) {
     if (n_rows <= 0) return BMC_OK;
-    block_scan_kernel<double><<<(n_rows + 63) / 64, 64, 0, st>>>(rec, n_rows, n_ev, stride, seg);
+    block_scan_kernel<double><<<(n_rows + kBlockScanRows - 1) / kBlockScanRows, kBlockScanThreads, 0, st>>>(
+        rec, n_rows, n_ev, stride, seg);
     CUDA_TRY(cudaGetLastError());
     return BMC_OK;
 }
@@ -322,21 +323,21 @@ bmc_status launch_adjoint(const ChainArgs& a, const int* row_ev, int n_tan, cons
     return BMC_OK;
 }
 
-template <int NC>
+template <int NC, bool kTan = true>
 bmc_status launch_adjoint_block(const ChainArgs& a, const int4* blk, int n_tan, const TaylorTable* tt, cudaStream_t st) {
     const size_t smem = kAdjBlkWarps * DenseGroup<NC>::G * sizeof(AdjBlkSlot<NC>);
     static std::atomic<unsigned long long> configured{0};
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
     if (dev >= 64 || !((configured.load(std::memory_order_acquire) >> dev) & 1ull)) {
-        CUDA_TRY(cudaFuncSetAttribute(adjoint_block_kernel<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        CUDA_TRY(cudaFuncSetAttribute(adjoint_block_kernel<NC, kTan>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
         if (dev < 64) configured.fetch_or(1ull << dev, std::memory_order_acq_rel);
     }
     const long long blocks = (a.n_chains + kAdjBlkWarps * 32 - 1) / (kAdjBlkWarps * 32);
     if (blocks > 0x7fffffffLL) return fail(BMC_ERR_INVALID, "%lld chains exceed one launch", a.n_chains);
     if (blocks == 0) return BMC_OK;
-    adjoint_block_kernel<NC><<<(unsigned)blocks, kAdjBlkWarps * 32, smem, st>>>(a, blk, n_tan, tt);
+    adjoint_block_kernel<NC, kTan><<<(unsigned)blocks, kAdjBlkWarps * 32, smem, st>>>(a, blk, n_tan, tt);
     CUDA_TRY(cudaGetLastError());
     return BMC_OK;
 }
@@ -466,12 +467,15 @@ struct Impl {
             CUDA_TRY(cub::DeviceRadixSort::SortPairs(t, tmp, k_in, k_out, i_in, i_out, (int)nch, 0, 32, st));
             a.order = i_out;
         }
-        if (!tg) return launch_chain<NC, double, 0, true>(a, tt, st);
+        // the plan's primal passes: the block kernel's layout without tangents where its rows qualify
+        // (forward mode keeps the chain kernel for them too)
+        const bool adj = pl.adj_ok && g_tangent_mode.load(std::memory_order_relaxed) == BMC_TANGENTS_AUTO;
+        if (!tg) return adj ? launch_adjoint_block<NC, false>(a, pl.adj_blk, 0, tt, st)
+                            : launch_chain<NC, double, 0, true>(a, tt, st);
         for (int t = 0; t < tg->n_tangents; ++t) a.field_row[t] = tg->field_row[t];
         a.seed = tg->d_seed;
         a.dm0 = tg->d_dm0;
-        if (pl.adj_ok && tg->n_tangents >= 2 && g_tangent_mode.load(std::memory_order_relaxed) == BMC_TANGENTS_AUTO)
-            return launch_adjoint_block<NC>(a, pl.adj_blk, tg->n_tangents, tt, st);
+        if (adj && tg->n_tangents >= 2) return launch_adjoint_block<NC, true>(a, pl.adj_blk, tg->n_tangents, tt, st);
         return run_tangents<NC, true>(a, tg->n_tangents, tt, st);
     }
 
@@ -920,8 +924,8 @@ bmc_status bmc_uneven_create(int32_t n_cest, int32_t n_voxels, const int32_t* h_
     }
     for (int t = 0; t < nt; ++t) {
         if (e == cudaSuccess && nev[t] > 0)
-            block_scan_kernel<double><<<(noff[t] + 63) / 64, 64>>>(pl->rec + base[t], noff[t], nev[t], noff[t],
-                                                                   pl->seg + row0[t]);
+            block_scan_kernel<double><<<(noff[t] + kBlockScanRows - 1) / kBlockScanRows, kBlockScanThreads>>>(
+                pl->rec + base[t], noff[t], nev[t], noff[t], pl->seg + row0[t]);
         else if (e == cudaSuccess)
             e = cudaMemset(pl->seg + row0[t], 0, sizeof(int4) * noff[t]);
     }

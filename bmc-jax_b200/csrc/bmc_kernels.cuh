@@ -723,15 +723,25 @@ __device__ __forceinline__ bool same_rec(const EvRec<R>& x, const EvRec<R>& y) {
     return x.dt == y.dt && x.w1 == y.w1 && x.c == y.c && x.s == y.s && x.wf == y.wf && x.type == y.type;
 }
 
+// One thread per (row, block length): kBlockScanRows rows of kBlockMaxL threads per block. Each thread
+// walks its row for its own L (the candidates at increasing start, the first largest saving kept);
+// the row's first thread then takes the largest saving over L = 1 .. kBlockMaxL in that order, so ties
+// go to the shortest block and then the earliest start.
+constexpr int kBlockScanRows = 16;
+constexpr int kBlockScanThreads = kBlockScanRows * kBlockMaxL;
+
 template <typename R>
-__global__ void block_scan_kernel(const EvRec<R>* __restrict__ ev, int n_rows, int n_ev, int stride,
-                                  int4* __restrict__ seg) {
-    const int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= n_rows) return;
-    const EvRec<R>* row = ev + o;
+__global__ void __launch_bounds__(kBlockScanThreads) block_scan_kernel(const EvRec<R>* __restrict__ ev, int n_rows,
+                                                                       int n_ev, int stride, int4* __restrict__ seg) {
+    __shared__ long long sv[kBlockScanThreads];
+    __shared__ int4 sb[kBlockScanThreads];
+    const int tid = threadIdx.x;
+    const int o = blockIdx.x * kBlockScanRows + tid / kBlockMaxL;
+    const int L = tid % kBlockMaxL + 1;
     int4 best = make_int4(0, 0, 0, 0);
     long long best_save = 0;
-    for (int L = 1; L <= kBlockMaxL; ++L) {
+    if (o < n_rows) {
+        const EvRec<R>* row = ev + o;
         int a = 0;
         while (a + 2 * L <= n_ev) {
             int r = 1;
@@ -761,7 +771,19 @@ __global__ void block_scan_kernel(const EvRec<R>* __restrict__ ev, int n_rows, i
             a += r * L;
         }
     }
-    seg[o] = best;
+    sv[tid] = best_save;
+    sb[tid] = best;
+    __syncthreads();
+    if (o < n_rows && L == 1) {
+        long long bs = 0;
+        int4 bb = make_int4(0, 0, 0, 0);
+        for (int l = 0; l < kBlockMaxL; ++l)
+            if (sv[tid + l] > bs) {
+                bs = sv[tid + l];
+                bb = sb[tid + l];
+            }
+        seg[o] = bb;
+    }
 }
 
 // ------------------------------------------------------------------------------------------------
