@@ -365,6 +365,15 @@ def run_ours(args, rank, world, local_rank):
                      "frac_fp64_equivalent": achieved / best if best else None,
                      "taylor_terms": terms, "taylor_terms_float32": terms32, "taylor_terms_executed": executed,
                      "dense_columns": hcols, "dense_squarings": squar,
+                     # the reference's work for the same result: one dense Pade-13 exponential of the
+                     # augmented matrix per event and chain (6 products and an LU solve with NA right-hand
+                     # sides, (6 + 4/3) 2 NA^3 FLOPs; its squarings left out, so a lower bound)
+                     "reference_equivalent": {
+                         "what": f"dense Pade-13 expm of the {NA}x{NA} augmented matrix per event (no squarings: "
+                                 "a lower bound), as simulation/expm.py computes it",
+                         "flops_per_event": (6 + 4 / 3) * 2 * NA ** 3,
+                         "events_per_launch": nv * n_off * n_ev,
+                         "tflops": (6 + 4 / 3) * 2 * NA ** 3 * nv * n_off * n_ev / (ms * 1e-3) / 1e12},
                      "peak_source": ("measured in this run: FMA-chain probe kernel (bmc_probe_fma_peak), burst; "
                                      "peak = the two pipes' peaks weighted by this launch's FLOPs on each "
                                      "(time of the FP64 share at the FP64 peak plus the FP32 share at the "

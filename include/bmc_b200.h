@@ -166,7 +166,10 @@ bmc_status bmc_simulate_trajectory(const bmc_problem* prob, const double* d_para
  * resets the state before the row ends: the CW Z-spectra and B1 ladders -- and two or more tangents are
  * asked for, one launch computes the Frechet derivative of that event's exponential in the readout's
  * direction, and every tangent follows from it (reverse mode through the exponential). The results agree
- * to rounding (~1e-12 relative). bmc_lm_fit chooses the same way. Choosing reads one flag back from
+ * to rounding (~1e-12 relative). bmc_lm_fit chooses the same way. An uneven plan (bmc_uneven_create)
+ * decides once when it is built: where every row's evolving events are one block of at most two events
+ * repeated at most 64 times (or at most two events once), its tangents and its primal passes both go
+ * through the block kernel (no read-back, so also inside a captured graph). Choosing reads one flag back from
  * the device (a stream synchronisation), so a stream being captured into a CUDA graph keeps forward
  * mode. bmc_set_tangent_mode(BMC_TANGENTS_FORWARD) makes forward mode the only one (process-wide);
  * BMC_TANGENTS_AUTO (the default) restores the choice.
