@@ -785,7 +785,7 @@ def run_dictionary(args, rank, world, local_rank):
     import bmc_oracle as O
     torch.cuda.set_device(local_rank)
     p, ev, m0, mz, grid = dictionary_model()
-    settings.use_x64(args.precision == "f64")
+    settings.use_precision(args.precision)
     try:
         generate_dictionary(p, ev, m0, {k: v[:2] for k, v in grid.items()}, mz)      # warm-up
         torch.cuda.synchronize()
@@ -795,7 +795,7 @@ def run_dictionary(args, rank, world, local_rank):
             entries, fp = generate_dictionary(p, ev, m0, grid, mz, chunk_size=262144)
             times.append(time.perf_counter() - t0)
     finally:
-        settings.use_x64(True)
+        settings.use_precision("f64")
     n = fp.shape[0]
     s = float(np.median(times))
     rng = np.random.default_rng(31)
