@@ -96,8 +96,11 @@ class _Group:
         if any(int(e.mz_loc) != mz for e in exps):
             raise ValueError(f"voxels with {nc} CEST pools disagree on mz_loc")
         keys, tables, vt = {}, [], []
+        by_obj = {}                                   # id -> key: a table object shared by voxels is hashed once
         for e in exps:
-            k = _table_key(e.events)
+            k = by_obj.get(id(e.events))
+            if k is None:
+                k = by_obj[id(e.events)] = _table_key(e.events)
             if k not in keys:
                 keys[k] = len(tables)
                 tables.append(e.events)
