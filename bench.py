@@ -1155,6 +1155,19 @@ def run_lmtangent(args, rank, world, local_rank):
             "roofline": r}
 
 
+def run_mlp(args, rank, world, local_rank):
+    """The warm-start network's tcgen05 GEMMs alone (mlp_roofline on the five-pool ladder's shape,
+    244 -> 3 x 256 -> 6): training steps at batch 4,096 replayed from a CUDA graph, --steps of them."""
+    import torch
+    torch.cuda.set_device(local_rank)
+    r = mlp_roofline(244, 6, steps=max(1, args.steps))
+    return {"metric": "warm-start network training step", "value": r["train_step_ms"], "unit": "ms",
+            "n_gpus": world, "steps": max(1, args.steps), "warmup": 1, "ms_per_step": r["train_step_ms"],
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
+            "data": "synthetic (random network and batch)",
+            "config": {"workload": "MLP 244 -> 3 x 256 (GELU) -> 6, batch 4096, Adam"}, "roofline": r}
+
+
 def run_warmfit(args, rank, world, local_rank):
     """The warm-vs-plain fit (warm_vs_plain) as its own bench line."""
     r = warm_vs_plain(args, rank, local_rank)
@@ -1174,7 +1187,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["forward", "fit", "warmfit", "lmtangent", "dictionary", "uneven",
+    ap.add_argument("--workload", choices=["forward", "fit", "warmfit", "lmtangent", "dictionary", "uneven", "mlp",
                                            "phantom08", "phantom09", "phantom10", "phantom11"],
                     default="forward")
     ap.add_argument("--train", type=int, default=2_000_000, help="warmfit: simulated training spectra")
@@ -1210,7 +1223,7 @@ def main():
             print(json.dumps(run_phantom(args)), flush=True)
         return
     run = {"fit": run_fit, "warmfit": run_warmfit, "lmtangent": run_lmtangent, "dictionary": run_dictionary,
-           "uneven": run_uneven}.get(args.workload, run_ours)
+           "uneven": run_uneven, "mlp": run_mlp}.get(args.workload, run_ours)
     line = run(args, rank, world, local_rank)
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -24,7 +24,7 @@ SLOT_SPREAD_SIGMA, SLOT_M_START = -2, -3
 TANGENTS_AUTO, TANGENTS_FORWARD = 0, 1
 
 EXPORTS = ("bmc_abi_version", "bmc_version", "bmc_last_error", "bmc_release", "bmc_simulate",
-           "bmc_simulate_jvp", "bmc_simulate_trajectory", "bmc_lm_fit", "bmc_normal_blocks",
+           "bmc_simulate_jvp", "bmc_simulate_design_jvp", "bmc_simulate_trajectory", "bmc_lm_fit", "bmc_normal_blocks",
            "bmc_simulate_counted", "bmc_simulate_jvp_counted", "bmc_probe_fma_peak", "bmc_simulate_noalloc",
            "bmc_mlp_sizes", "bmc_mlp_sync", "bmc_mlp_forward", "bmc_mlp_backward", "bmc_mlp_adam_step",
            "bmc_mlp_adam_step_dev", "bmc_uneven_create", "bmc_uneven_simulate",
@@ -92,6 +92,9 @@ def lib():
         L.bmc_simulate_jvp.argtypes = [C.POINTER(Problem), vp, C.POINTER(Events), vp, C.POINTER(Spread),
                                        C.POINTER(Tangents), vp, vp, vp]
         L.bmc_simulate_jvp.restype = C.c_int
+        L.bmc_simulate_design_jvp.argtypes = [C.POINTER(Problem), vp, C.POINTER(Events), vp, vp, C.POINTER(Events), vp,
+                                              C.POINTER(Tangents), vp, vp, vp, vp, vp]
+        L.bmc_simulate_design_jvp.restype = C.c_int
         L.bmc_simulate_trajectory.argtypes = [C.POINTER(Problem), vp, C.POINTER(Events), vp, vp, vp]
         L.bmc_simulate_trajectory.restype = C.c_int
         L.bmc_lm_fit.argtypes = [C.POINTER(Problem), vp, C.POINTER(Events), vp, C.POINTER(Spread),

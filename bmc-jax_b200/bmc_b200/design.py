@@ -13,7 +13,8 @@ from .fitting import FitSpec, field_row, write_params
 from .simulation import (SimEvent, n_cest_of, n_samples, pack_params, state_size, DeviceEvents, problem,
                          _device)
 
-__all__ = ["crlb", "CRLB", "fisher_information", "model_of", "jacobian", "optimize_design", "DesignResult"]
+__all__ = ["crlb", "CRLB", "fisher_information", "model_of", "jacobian", "optimize_design", "DesignResult",
+           "design_cost", "design_cost_and_gradient", "design_jacobians"]
 
 
 def _check(experiment, spec: FitSpec):
@@ -160,17 +161,117 @@ def design_cost(build: Callable, spec: FitSpec, d, sigma: float, truths, targets
     return total / truths.shape[0]
 
 
+_EV_FIELDS = ("dt", "rf_amp", "rf_phase", "rf_freq")
+
+
+def _build_direction(build: Callable, d, i: int, h: float, ref):
+    """The derivative of build(d) with respect to setting i: (events, packed params [n_fields], m0) per unit
+    of d_i, by the five-point stencil (-f(+2h) + 8 f(+h) - 8 f(-h) + f(-2h)) / 12h of the host build,
+    which is exact to rounding wherever build is affine in d_i (amplitudes, durations and offsets scaled
+    or shifted by a setting), O(h^4) otherwise. Everything after the build is differentiated exactly."""
+    pts = {}
+    for k in (-2, -1, 1, 2):
+        dd = np.array(d, np.float64, copy=True)
+        dd[i] += k * h
+        ex = build(dd)
+        ev = ex.events
+        if np.shape(ev.dt) != np.shape(ref.events.dt) or not np.array_equal(np.asarray(ev.type),
+                                                                          np.asarray(ref.events.type)):
+            raise ValueError(f"build(d) must keep the event table's shape and event types as setting {i} moves")
+        if int(ex.mz_loc) != int(ref.mz_loc) or n_cest_of(ex.params) != n_cest_of(ref.params):
+            raise ValueError(f"build(d) must keep the pools and mz_loc as setting {i} moves")
+        pts[k] = ([np.asarray(getattr(ev, f), np.float64) for f in _EV_FIELDS], pack_params(ex.params, 1)[:, 0],
+                  np.asarray(ex.m0, np.float64).reshape(-1))
+    st = lambda a2, a1, m1, m2: (-a2 + 8.0 * a1 - 8.0 * m1 + m2) / (12.0 * h)
+    ev = [st(pts[2][0][j], pts[1][0][j], pts[-1][0][j], pts[-2][0][j]) for j in range(len(_EV_FIELDS))]
+    return ev, st(pts[2][1], pts[1][1], pts[-1][1], pts[-2][1]), st(pts[2][2], pts[1][2], pts[-1][2], pts[-2][2])
+
+
+def design_jacobians(build: Callable, spec: FitSpec, d, X_phys, steps):
+    """(J, dJ) at design d: J = dZ/dx (physical units) at every row of X_phys, (n, n_offsets, P), and dJ its
+    derivative with respect to every setting of d, (len(d), n, n_offsets, P), from the second-order kernel
+    (bmc_simulate_design_jvp: forward mode over forward mode through the whole simulation, one launch per
+    tangent and setting). `steps[i]` is the stencil step that differentiates the host build in d_i
+    (_build_direction). The fitted fields are set by x, so the design moves only the others."""
+    from .simulation import tile_params
+    torch = _lib.torch_cuda()
+    d = np.asarray(d, np.float64)
+    exp = build(d)
+    _check(exp, spec)
+    X = np.atleast_2d(np.asarray(X_phys, np.float64))
+    n = X.shape[0]
+    nc = n_cest_of(exp.params)
+    N = state_size(nc)
+    P = spec.n
+    rows = [field_row(sl.field, sl.index, nc) for sl in spec.slots]
+    p = write_params(tile_params(exp.params, n), X / spec.scales, spec)
+    dev_ev = DeviceEvents(exp.events)
+    n_off = dev_ev.n_offsets
+    pdev = _device(pack_params(p, n))
+    mdev = _device(np.broadcast_to(np.asarray(exp.m0, np.float64).reshape(1, -1), (n, N)))
+    tg = _lib.Tangents()
+    tg.n_tangents = P
+    for t, r in enumerate(rows):
+        tg.field_row[t] = r
+    seed = _device(np.ones((P, n)))
+    tg.d_seed = seed.data_ptr()
+    tg.d_dm0 = None
+    pr = problem(n, n_off, dev_ev.n_events, nc, int(exp.mz_loc), _lib.F64)
+    f64 = dict(dtype=torch.float64, device="cuda")
+    z, jz = torch.empty((n, n_off), **f64), torch.empty((P, n, n_off), **f64)
+    dz, djz = torch.empty((n, n_off), **f64), torch.empty((P, n, n_off), **f64)
+    J, dJ = None, np.empty((d.size, n, n_off, P))
+    for i in range(d.size):
+        ev_d, p_d, m_d = _build_direction(build, d, i, float(steps[i]), exp)
+        p_d = np.repeat(p_d.reshape(-1, 1), n, axis=1)
+        p_d[rows] = 0.0
+        evd = [_device(a) for a in ev_d]
+        ev_struct = _lib.Events(0, evd[0].data_ptr(), evd[1].data_ptr(), evd[2].data_ptr(), evd[3].data_ptr(), 0)
+        pd_dev = _device(p_d)
+        md_dev = _device(np.broadcast_to(m_d.reshape(1, -1), (n, N)))
+        _lib.check(_lib.lib().bmc_simulate_design_jvp(pr, _lib.ptr(pdev), dev_ev.struct, _lib.ptr(mdev),
+                                                      _lib.ptr(pd_dev), ev_struct, _lib.ptr(md_dev), tg, _lib.ptr(z),
+                                                      _lib.ptr(jz), _lib.ptr(dz), _lib.ptr(djz),
+                                                      _lib.stream_handle()))
+        if J is None:
+            J = jz.cpu().numpy().transpose(1, 2, 0)
+        dJ[i] = djz.cpu().numpy().transpose(1, 2, 0)
+    return J, dJ
+
+
+def design_cost_and_gradient(build: Callable, spec: FitSpec, d, sigma: float, truths, targets: Sequence[str],
+                             steps):
+    """(cost, d cost / d d): the cost of design_cost and its exact gradient. With F = J^T J / sigma^2 and
+    var = diag(F^-1), a setting's dJ gives dF = (dJ^T J + J^T dJ) / sigma^2 and d var = -diag(F^-1 dF F^-1)."""
+    names = [sl.name for sl in spec.slots]
+    idx = np.array([names.index(t) for t in targets])
+    truths = np.atleast_2d(np.asarray(truths, np.float64))
+    J, dJ = design_jacobians(build, spec, d, truths, steps)
+    cost, grad = 0.0, np.zeros(dJ.shape[0])
+    for k, x in enumerate(truths):
+        Jx = J[k]
+        Fi = np.linalg.inv(Jx.T @ Jx / sigma ** 2)
+        w = 1.0 / x[idx] ** 2
+        cost += float(np.sum(np.diag(Fi)[idx] * w))
+        for i in range(dJ.shape[0]):
+            dF = (dJ[i, k].T @ Jx + Jx.T @ dJ[i, k]) / sigma ** 2
+            grad[i] -= float(np.sum(np.diag(Fi @ dF @ Fi)[idx] * w))
+    return cost / truths.shape[0], grad / truths.shape[0]
+
+
 def optimize_design(build: Callable, spec: FitSpec, d0, lo, hi, sigma: float, truths,
                     targets: Optional[Sequence[str]] = None, n_steps: int = 200, lr: float = 0.05,
-                    callback: Optional[Callable] = None, rel_step: float = 1e-4) -> DesignResult:
+                    callback: Optional[Callable] = None, rel_step: float = 1e-3) -> DesignResult:
     """Lower the Cramer-Rao bound of the target parameters by changing the design (design/optimize.py:43-113).
 
     `build(d) -> Experiment` (one sample) from a design vector d, here with NumPy operations. The cost,
     its parametrisation d = lo + (hi - lo) sigmoid(u) and the Adam steps on u are the reference's. The
     reference differentiates the cost with respect to d by automatic differentiation through the bound;
-    here the Jacobian inside the bound is the exact forward-mode tangent of the GPU kernel and the outer
-    derivative is a central difference in each setting with step rel_step * (hi - lo): 2 len(d) + 1
-    bound evaluations (one launch each, every truth in it) per step, float64 throughout."""
+    here the gradient is exact from the simulation on: the second-order kernel (bmc_simulate_design_jvp)
+    carries each setting's direction and every parameter tangent through the whole simulation at once
+    (design_cost_and_gradient). NumPy cannot be traced, so the build itself is differentiated by a
+    five-point stencil with step rel_step * (hi - lo) (exact to rounding for builds affine in each
+    setting, such as scaled amplitudes). float64 throughout."""
     names = [sl.name for sl in spec.slots]
     targets = tuple(names if targets is None else targets)
     unknown = [t for t in targets if t not in names]
@@ -190,12 +291,7 @@ def optimize_design(build: Callable, spec: FitSpec, d0, lo, hi, sigma: float, tr
     history = []
     for step in range(int(n_steps)):
         d = to_d(u)
-        c = cost_of(d)
-        gd = np.empty_like(d)
-        for i in range(d.size):
-            e = np.zeros_like(d)
-            e[i] = h[i]
-            gd[i] = (cost_of(d + e) - cost_of(d - e)) / (2.0 * h[i])
+        c, gd = design_cost_and_gradient(build, spec, d, sigma, truths, targets, h)
         g = gd * (hi - lo) * sig(u) * (1.0 - sig(u))
         if not (np.isfinite(c) and np.all(np.isfinite(g))):
             raise FloatingPointError(f"cost or gradient not finite at step {step}; try a smaller lr")

@@ -24,6 +24,7 @@
 #include "bmc_joint.cuh"
 #include "bmc_adjoint.cuh"
 #include "bmc_adjoint_block.cuh"
+#include "bmc_design.cuh"
 
 using namespace bmc;
 
@@ -118,6 +119,36 @@ void host_tables(TaylorTable* h) {
     h[BMC_F64] = make_table(1e-13, 30, 0.5, 100.0, 1e-6);
     h[BMC_F32] = make_table(std::ldexp(1.0, -24), 16, 0.5, 100.0, 0.0);
     h[BMC_MIXED] = make_table(BMC_MIXED_TOL, 30, 0.5, 100.0, BMC_MIXED_F32);
+}
+
+// The host copy of one of the library's device tables: the chain kernel takes its table by value, as a
+// kernel parameter, so that the loads of the Taylor loops with warp-uniform indices come from the
+// constant bank. `tt` must point into g_tables (as tables() and noalloc_setup() return).
+bmc_status host_table_of(const TaylorTable* tt, TaylorTable* out) {
+    static TaylorTable h[3];
+    static std::once_flag once;
+    std::call_once(once, [] { host_tables(h); });
+    // the device address of g_tables, looked up once per device (a call under stream capture then
+    // makes no runtime query)
+    static std::mutex mu;
+    static std::map<int, const TaylorTable*> bases;
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    const TaylorTable* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = bases.find(dev);
+        if (it == bases.end()) {
+            TaylorTable* b = nullptr;
+            CUDA_TRY(cudaGetSymbolAddress((void**)&b, g_tables));
+            it = bases.emplace(dev, b).first;
+        }
+        base = it->second;
+    }
+    const long long i = tt - base;
+    if (i < 0 || i > 2) return fail(BMC_ERR_INVALID, "Taylor table %p is not one of the library's", (const void*)tt);
+    *out = h[i];
+    return BMC_OK;
 }
 
 struct DeviceState {
@@ -295,7 +326,9 @@ bmc_status launch_chain(const ChainArgs& a, const TaylorTable* tt, cudaStream_t 
     const long long blocks = (nch + kWarps * 32 - 1) / (kWarps * 32);
     if (blocks > 0x7fffffffLL) return fail(BMC_ERR_INVALID, "%lld chains exceed one launch", nch);
     if (blocks == 0) return BMC_OK;
-    chain_kernel<NC, R, NT, U><<<(unsigned)blocks, kWarps * 32, smem, st>>>(a, tt);
+    TaylorTable th;
+    if (bmc_status s = host_table_of(tt, &th); s != BMC_OK) return s;
+    chain_kernel<NC, R, NT, U><<<(unsigned)blocks, kWarps * 32, smem, st>>>(a, th);
     CUDA_TRY(cudaGetLastError());
     return BMC_OK;
 }
@@ -576,6 +609,55 @@ struct Impl {
         return run_tangents<NC>(a, tg->n_tangents, tt, st);
     }
 
+    // Z, its tangents and the derivatives of both along one design direction (design_kernel): one launch
+    // per tangent, the direction's records prepared beside the table's
+    static bmc_status design(const bmc_problem* pr, const double* params, const bmc_events* ev, const double* m0,
+                             const double* params_dir, const bmc_events* ev_dir, const double* m0_dir,
+                             const bmc_tangents* tg, double* z, double* jz, double* dz, double* djz, cudaStream_t st) {
+        const TaylorTable* tt = nullptr;
+        bmc_status s = tables(BMC_F64, &tt);
+        if (s != BMC_OK) return s;
+        const size_t nrec = (size_t)pr->n_offsets * pr->n_events;
+        const long long nch = (long long)pr->n_voxels * pr->n_offsets;
+        const size_t mats = (size_t)nch * (2 * N * N + N);           // Phi, its square, psi per chain
+        void* ws = nullptr;
+        if ((s = workspace(2 * align256(nrec * sizeof(EvRec<double>)) + 256 + align256(mats * sizeof(Dn<HD, 1>)),
+                           st, &ws)) != BMC_OK)
+            return s;
+        Carve cv(ws);
+        ChainArgs a{};
+        a.n_vox = pr->n_voxels; a.n_off = pr->n_offsets; a.n_ev = pr->n_events; a.n_fields = Layout<NC>::NF;
+        a.mz = pr->mz_loc; a.reset_after_adc = pr->reset_after_adc;
+        if ((s = fill_spread(a, nullptr)) != BMC_OK) return s;
+        a.params = params; a.params_dir = params_dir; a.m0 = m0; a.out = z; a.jout = jz;
+        for (int t = 0; t < tg->n_tangents; ++t) a.field_row[t] = tg->field_row[t];
+        a.seed = tg->d_seed;
+        a.status = cv.take<int>(1);
+        CUDA_TRY(cudaMemsetAsync(a.status, 0, sizeof(int), st));
+        EvRec<double>* rec = cv.take<EvRec<double>>(nrec);
+        if ((s = prep_events<double>(pr, ev, rec, st)) != BMC_OK) return s;
+        a.ev = rec;
+        DesignArgs d{};
+        if (ev_dir && nrec > 0) {
+            EvRec<double>* dr = cv.take<EvRec<double>>(nrec);
+            const int blocks = (int)std::min<size_t>((nrec + 255) / 256, 148 * 16);
+            prep_dir_kernel<<<blocks, 256, 0, st>>>(pr->n_offsets, pr->n_events, ev->d_rf_phase, ev_dir->d_dt,
+                                                   ev_dir->d_rf_amp, ev_dir->d_rf_phase, ev_dir->d_rf_freq, dr);
+            CUDA_TRY(cudaGetLastError());
+            d.ev_dir = dr;
+        }
+        d.m0_dir = m0_dir; d.dz = dz; d.djz = djz;
+        d.scratch = reinterpret_cast<double*>(cv.take<Dn<HD, 1>>(mats));
+        const long long blocks = (nch + 127) / 128;
+        if (blocks > 0x7fffffffLL) return fail(BMC_ERR_INVALID, "%lld chains exceed one launch", nch);
+        for (int t = 0; t < tg->n_tangents; ++t) {
+            a.t0 = t;
+            design_kernel<NC, 1><<<(unsigned)blocks, 128, 0, st>>>(a, d, tt);
+            CUDA_TRY(cudaGetLastError());
+        }
+        return BMC_OK;
+    }
+
     static bmc_status lm(const bmc_problem* pr, const double* params, const bmc_events* ev, const double* m0,
                          const bmc_spread* sp, const bmc_fit_spec* fs, const double* zm, const double* x0,
                          double* x_out, double* cost_traj, double* x_traj, cudaStream_t st) {
@@ -807,6 +889,21 @@ bmc_status bmc_simulate_jvp(const bmc_problem* prob, const double* d_params, con
         if (tan->field_row[t] >= nf || tan->field_row[t] < BMC_SEED_SPREAD_SIGMA)
             return fail(BMC_ERR_INVALID, "tangent %d: field row %d outside -2..%d", t, tan->field_row[t], nf - 1);
     BMC_DISPATCH(prob->n_cest, jvp(prob, d_params, ev, d_m0, spread, tan, d_z, d_jz, (cudaStream_t)stream));
+}
+
+bmc_status bmc_simulate_design_jvp(const bmc_problem* prob, const double* d_params, const bmc_events* ev,
+                                   const double* d_m0, const double* d_params_dir, const bmc_events* ev_dir,
+                                   const double* d_m0_dir, const bmc_tangents* tan, double* d_z, double* d_jz,
+                                   double* d_dz, double* d_djz, void* stream) {
+    bmc_status s = check_jvp(prob, d_params, ev, d_m0, tan, d_z, d_jz);
+    if (s != BMC_OK) return s;
+    if (!d_dz || !d_djz) return fail(BMC_ERR_INVALID, "null design-derivative output");
+    if (tan->d_dm0) return fail(BMC_ERR_UNSUPPORTED, "bmc_simulate_design_jvp: start-state tangents (d_dm0)");
+    for (int t = 0; t < tan->n_tangents; ++t)
+        if (tan->field_row[t] < 0)
+            return fail(BMC_ERR_UNSUPPORTED, "bmc_simulate_design_jvp: tangent %d seeds the spread (no spread here)", t);
+    BMC_DISPATCH(prob->n_cest, design(prob, d_params, ev, d_m0, d_params_dir, ev_dir, d_m0_dir, tan, d_z, d_jz, d_dz,
+                                      d_djz, (cudaStream_t)stream));
 }
 
 bmc_status bmc_lm_fit(const bmc_problem* prob, const double* d_params, const bmc_events* ev, const double* d_m0,

@@ -42,6 +42,7 @@ struct ChainArgs {
     int n_nodes;               // spread isochromats (1 = none)
     double u[kMaxNodes], w[kMaxNodes];
     const double* params;      // [n_fields][n_vox]
+    const double* params_dir;  // [n_fields][n_vox] or null: the design direction of params (design kernel)
     const void* ev;            // EvRec<R>[n_ev][n_off]
     const double* m0;          // [n_vox][N]
     const double* sigma;       // [n_vox] spread width [Hz] or null
@@ -102,7 +103,7 @@ struct Chain {
     // tangents t0 .. t0 + NT - 1 of the launch's set (a.t0 in the chain kernel; the adjoint kernel seeds
     // one tangent per lane)
     static __device__ __forceinline__ D field(const ChainArgs& a, int row, int v, int t0) {
-        D r = dconst<R, NT>(R(a.params[(size_t)row * a.n_vox + v]));
+        D r = dconst<R, NT>(lift<R>(a.params, a.params_dir, (size_t)row * a.n_vox + v));
         if constexpr (NT > 0) {
 #pragma unroll
             for (int t = 0; t < NT; ++t)
@@ -200,7 +201,7 @@ struct Chain {
     static __device__ __forceinline__ R hyp(R a, R b) { return fmax(a, b) + R(0.41421357) * fmin(a, b); }
     // sqrt(a^2 + b^2), rounded; the callers scale their result by (1 + kNormSlack) to keep a bound
     static __device__ __forceinline__ R blk(R a, R b) { return sqrt(fma(a, a, b * b)); }
-    static constexpr double kNormSlack = sizeof(R) == 8 ? 1e-14 : 1e-6;
+    static constexpr double kNormSlack = std::is_same<R, float>::value ? 1e-6 : 1e-14;
 
     // An upper bound of ||D^-1 A D|| in the norm max_b ||v_b||_2 / d_b over blocks b = (x, y) pairs and
     // z entries, with d = sqrt(f) per pool. The similarity balances the exchange terms (detailed

@@ -150,6 +150,68 @@ __device__ __forceinline__ Dn<R, NT> dabs(Dn<R, NT> a) {
     return a.v >= R(0) ? a : -a;
 }
 
+// ------------------------------------------------------------------------------------------------
+// HD: a float64 value with its derivative along one direction of the inputs (a design setting that
+// moves the event table, the parameters and the start state together). Used as the scalar of the dual
+// numbers, Dn<HD, NT> carries a quantity, its NT parameter tangents, and the derivative of each along
+// the design direction: the mixed second derivatives of forward mode over forward mode. Values are
+// computed exactly as in float64 (division and square root included), so the value parts of a
+// Dn<HD, NT> computation are those of the Dn<double, NT> one. Comparisons look at the value only.
+// ------------------------------------------------------------------------------------------------
+// the global math functions stay visible beside HD's overloads below
+using ::exp;
+using ::fabs;
+using ::fma;
+using ::fmax;
+using ::fmin;
+using ::sqrt;
+
+struct HD {
+    double v, e;
+    HD() = default;
+    __host__ __device__ constexpr HD(double x) : v(x), e(0.0) {}
+    __host__ __device__ constexpr HD(double x, double dx) : v(x), e(dx) {}
+};
+__device__ __forceinline__ HD operator+(HD a, HD b) { return HD(a.v + b.v, a.e + b.e); }
+__device__ __forceinline__ HD operator-(HD a, HD b) { return HD(a.v - b.v, a.e - b.e); }
+__device__ __forceinline__ HD operator-(HD a) { return HD(-a.v, -a.e); }
+__device__ __forceinline__ HD operator*(HD a, HD b) { return HD(a.v * b.v, fma(a.v, b.e, a.e * b.v)); }
+__device__ __forceinline__ HD operator/(HD a, HD b) {
+    const double q = a.v / b.v;
+    return HD(q, (a.e - q * b.e) / b.v);
+}
+__device__ __forceinline__ HD& operator+=(HD& a, HD b) { return a = a + b; }
+__device__ __forceinline__ HD fma(HD a, HD b, HD c) {
+    return HD(fma(a.v, b.v, c.v), fma(a.v, b.e, fma(a.e, b.v, c.e)));
+}
+__device__ __forceinline__ HD fabs(HD a) { return a.v < 0.0 ? -a : a; }
+__device__ __forceinline__ HD fmax(HD a, HD b) { return (a.v >= b.v || b.v != b.v) ? a : b; }
+__device__ __forceinline__ HD fmin(HD a, HD b) { return (a.v <= b.v || b.v != b.v) ? a : b; }
+__device__ __forceinline__ HD sqrt(HD a) {
+    const double r = sqrt(a.v);
+    return HD(r, r > 0.0 ? a.e / (2.0 * r) : 0.0);
+}
+__device__ __forceinline__ HD exp(HD a) {
+    const double r = exp(a.v);
+    return HD(r, r * a.e);
+}
+__device__ __forceinline__ bool operator<(HD a, HD b) { return a.v < b.v; }
+__device__ __forceinline__ bool operator>(HD a, HD b) { return a.v > b.v; }
+__device__ __forceinline__ bool operator<=(HD a, HD b) { return a.v <= b.v; }
+__device__ __forceinline__ bool operator>=(HD a, HD b) { return a.v >= b.v; }
+__device__ __forceinline__ bool operator==(HD a, HD b) { return a.v == b.v; }
+__device__ __forceinline__ bool operator!=(HD a, HD b) { return a.v != b.v; }
+
+// element i of an input array as the scalar R: with HD, its design derivative from `dir` (null = 0)
+template <typename R>
+__device__ __forceinline__ R lift(const double* x, const double* dir, size_t i) {
+    return R(x[i]);
+}
+template <>
+__device__ __forceinline__ HD lift<HD>(const double* x, const double* dir, size_t i) {
+    return HD(x[i], dir ? dir[i] : 0.0);
+}
+
 
 // ------------------------------------------------------------------------------------------------
 // event records: the shared event table, preprocessed once per call (bmc_prep_events)

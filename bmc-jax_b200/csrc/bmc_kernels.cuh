@@ -449,7 +449,7 @@ __device__ __forceinline__ void convert_flat(const A& a, B& b) {
 // ------------------------------------------------------------------------------------------------
 template <int NC, typename R, int NT, bool UNEVEN = false>
 __global__ void __launch_bounds__(32 * ChainLaunch<NC, NT>::kWarps, ChainLaunch<NC, NT>::kMinBlocks)
-chain_kernel(const ChainArgs a, const TaylorTable* __restrict__ ttab) {
+chain_kernel(const ChainArgs a, const __grid_constant__ TaylorTable tt) {
     using D = Dn<R, NT>;
     using C = Chain<NC, R, NT>;
     using RD = typename DenseReal<R>::type;
@@ -458,7 +458,6 @@ chain_kernel(const ChainArgs a, const TaylorTable* __restrict__ ttab) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     SM* dsm = reinterpret_cast<SM*>(smem_raw) + (threadIdx.x >> 5);
-    const TaylorTable& tt = *ttab;
 
     // chains in offset-fastest order: neighbouring lanes are neighbouring offsets of one voxel, so a
     // warp shares parameters and its chains need similar Taylor orders

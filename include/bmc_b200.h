@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define BMC_ABI_VERSION 3
+#define BMC_ABI_VERSION 4
 #define BMC_MAX_CEST 5             /* water + up to five CEST pools + MT: N <= 19 */
 #define BMC_MAX_TANGENTS 8
 #define BMC_N_FIELDS(n_cest) (13 + 5 * (n_cest))
@@ -180,6 +180,25 @@ bmc_status bmc_set_tangent_mode(int32_t mode);
 bmc_status bmc_simulate_jvp(const bmc_problem* prob, const double* d_params, const bmc_events* ev,
                             const double* d_m0, const bmc_spread* spread, const bmc_tangents* tan,
                             double* d_z, double* d_jz, void* stream);
+
+/*
+ * Second-order tangents for protocol design. Replaces the derivative of the Cramer-Rao bound with
+ * respect to the design that design/optimize.py:43-113 takes by automatic differentiation through
+ * jax.jacfwd of the model (design/crlb.py:57): Z and its tangents as bmc_simulate_jvp computes them,
+ * plus the derivative of both along one direction of the inputs -- d_params_dir [n_fields][n_voxels]
+ * and d_m0_dir [n_voxels][N] (either NULL = 0), and ev_dir (NULL = 0), whose d_dt, d_rf_amp,
+ * d_rf_phase and d_rf_freq are the per-unit change of the table's fields ([n_offsets][n_events] like
+ * ev; NULL fields = 0; d_type and d_adc_idx are not read). d_dz: [n_voxels][n_offsets];
+ * d_djz: [n_tangents][n_voxels][n_offsets]. Exact derivatives of the computed approximation: every
+ * scalar of the chain carries its design derivative, every state entry its tangents (forward mode over
+ * forward mode); long events take a dense scaling and squaring per chain. float64, mz_loc >= 0, no
+ * spread, tangents of params fields only (no d_dm0). One launch per tangent; meant for the small
+ * problems of a design (truths x protocol rows), not for bulk simulation.
+ */
+bmc_status bmc_simulate_design_jvp(const bmc_problem* prob, const double* d_params, const bmc_events* ev,
+                                   const double* d_m0, const double* d_params_dir, const bmc_events* ev_dir,
+                                   const double* d_m0_dir, const bmc_tangents* tan, double* d_z, double* d_jz,
+                                   double* d_dz, double* d_djz, void* stream);
 
 /*
  * Bounded Levenberg-Marquardt of every voxel, all iterations on the device.
