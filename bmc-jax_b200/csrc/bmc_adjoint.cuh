@@ -298,7 +298,7 @@ struct Adjoint {
 #endif
 template <int NC, bool kTan>
 __global__ void __launch_bounds__(32 * kAdjWarps, kTan ? 2 : BMC_ADJ_PRIMAL_BLOCKS)
-adjoint_kernel(const ChainArgs a, const int* __restrict__ row_ev, int n_tan, const TaylorTable* __restrict__ ttab) {
+adjoint_kernel(const ChainArgs a, const int* __restrict__ row_ev, int n_tan, const __grid_constant__ TaylorTable tt) {
     using A = Adjoint<NC>;
     using D0 = Dn<double, 0>;
     using C0 = Chain<NC, double, 0>;
@@ -307,7 +307,6 @@ adjoint_kernel(const ChainArgs a, const int* __restrict__ row_ev, int n_tan, con
     constexpr int N = A::N, GS = A::GS, G = A::G, LD = A::LD, PHI_LANE = AdjGroup<NC>::PHI_LANE;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SL* slots = reinterpret_cast<SL*>(smem_raw) + (threadIdx.x >> 5) * G;
-    const TaylorTable& tt = *ttab;
     const int lane = threadIdx.x & 31, grp = lane / GS, gl = lane % GS;
 
     const long long nch = (long long)a.n_vox * a.n_off;

@@ -24,7 +24,9 @@ namespace bmc {
 constexpr int kAdjL = 2;      // block events the kernel takes
 constexpr int kAdjMaxR = 64;  // block repeats it takes
 
-template <int NC>
+// kTan false (the primal passes): the tangent-only members shrink to one element, so that the slot
+// leaves shared memory for more resident blocks
+template <int NC, bool kTan = true>
 struct AdjBlkSlotBody {
     static constexpr int N = Layout<NC>::N;
     static constexpr int NA = N + 1;
@@ -34,11 +36,11 @@ struct AdjBlkSlotBody {
     double C[NC + 2];                         // the constant column (water z, MT z, CEST z), unscaled
     double E[kAdjL][NA * LD];                 // the events' propagators
     double P[NA * LD];                        // the block propagator; then T of the Frechet squarings
-    double A[NA * LD];                        // W and its right products
-    double B[NA * LD];                        // W_i; then H of the Frechet squarings
+    double A[kTan ? NA * LD : 1];             // W and its right products
+    double B[kTan ? NA * LD : 1];             // W_i; then H of the Frechet squarings
     double vec[2][NA];
-    K dk[kAdjL][kMaxT];                       // per event and tangent: d(coefficients) * dt_i
-    double dC[kMaxT][NC + 2];                 // per tangent: d(constant column), unscaled
+    K dk[kAdjL][kTan ? kMaxT : 1];            // per event and tangent: d(coefficients) * dt_i
+    double dC[kTan ? kMaxT : 1][NC + 2];      // per tangent: d(constant column), unscaled
     double res[kMaxT + 1];
     EvRec<double> rec[kAdjL];
     double g0[kAdjL], gd[kAdjL][3], h[kAdjL], scale[kAdjL];
@@ -46,9 +48,9 @@ struct AdjBlkSlotBody {
     int L, r, vox;
 };
 
-template <int NC>
-struct AdjBlkSlot : AdjBlkSlotBody<NC> {
-    static constexpr size_t kBody = sizeof(AdjBlkSlotBody<NC>);
+template <int NC, bool kTan = true>
+struct AdjBlkSlot : AdjBlkSlotBody<NC, kTan> {
+    static constexpr size_t kBody = sizeof(AdjBlkSlotBody<NC, kTan>);
     static constexpr size_t kTarget = (128 / DenseGroup<NC>::G) % 128;
     static constexpr size_t kPad = (kTarget + 128 - kBody % 128) % 128;
     char pad[kPad == 0 ? 128 : kPad];
@@ -99,7 +101,7 @@ __global__ void adjoint_block_rows_kernel(const EvRec<double>* __restrict__ rec,
     if (!ok) atomicAnd(all_ok, 0);
 }
 
-template <int NC>
+template <int NC, bool kTan = true>
 struct AdjBlk {
     using D0 = Dn<double, 0>;
     using D1 = Dn<double, 1>;
@@ -107,7 +109,7 @@ struct AdjBlk {
     using C1 = Chain<NC, double, 1>;
     using S = State<NC, D0>;
     using K = StepCoef<NC, D0>;
-    using SL = AdjBlkSlot<NC>;
+    using SL = AdjBlkSlot<NC, kTan>;
     static constexpr int N = Layout<NC>::N;
     static constexpr int NA = N + 1;
     static constexpr int GS = DenseGroup<NC>::GS;
@@ -341,19 +343,22 @@ struct AdjBlk {
     }
 };
 
-// kTan false: z only (phases A, B and D without W), for the plan's primal passes
+// kTan false: z only (phases A, B and D without W), for the plan's primal passes, with a smaller slot and
+// registers capped for BMC_ADJ_BLK_PRIMAL_BLOCKS resident blocks (a build may set it for a sweep)
+#ifndef BMC_ADJ_BLK_PRIMAL_BLOCKS
+#define BMC_ADJ_BLK_PRIMAL_BLOCKS 3
+#endif
 template <int NC, bool kTan>
-__global__ void __launch_bounds__(32 * kAdjBlkWarps, 2)
-adjoint_block_kernel(const ChainArgs a, const int4* __restrict__ blk, int n_tan, const TaylorTable* __restrict__ ttab) {
-    using AB = AdjBlk<NC>;
+__global__ void __launch_bounds__(32 * kAdjBlkWarps, kTan ? 2 : BMC_ADJ_BLK_PRIMAL_BLOCKS)
+adjoint_block_kernel(const ChainArgs a, const int4* __restrict__ blk, int n_tan, const __grid_constant__ TaylorTable tt) {
+    using AB = AdjBlk<NC, kTan>;
     using D0 = Dn<double, 0>;
     using C0 = Chain<NC, double, 0>;
     using S = State<NC, D0>;
-    using SL = AdjBlkSlot<NC>;
+    using SL = AdjBlkSlot<NC, kTan>;
     constexpr int N = AB::N, NA = AB::NA, GS = AB::GS, G = AB::G, LD = AB::LD;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SL* slots = reinterpret_cast<SL*>(smem_raw) + (threadIdx.x >> 5) * G;
-    const TaylorTable& tt = *ttab;
     const int lane = threadIdx.x & 31, grp = lane / GS, gl = lane % GS;
 
     const long long nch = a.n_chains;

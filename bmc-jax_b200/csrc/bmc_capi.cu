@@ -121,8 +121,8 @@ void host_tables(TaylorTable* h) {
     h[BMC_MIXED] = make_table(BMC_MIXED_TOL, 30, 0.5, 100.0, BMC_MIXED_F32);
 }
 
-// The host copy of one of the library's device tables: the chain kernel takes its table by value, as a
-// kernel parameter, so that the loads of the Taylor loops with warp-uniform indices come from the
+// The host copy of one of the library's device tables: the chain and adjoint kernels take their table by
+// value, as a kernel parameter, so that the loads of the Taylor loops with warp-uniform indices come from the
 // constant bank. `tt` must point into g_tables (as tables() and noalloc_setup() return).
 bmc_status host_table_of(const TaylorTable* tt, TaylorTable* out) {
     static TaylorTable h[3];
@@ -307,8 +307,8 @@ __global__ void __launch_bounds__(256) fma_probe_kernel(int iters, R seed, R* si
 // ------------------------------------------------------------------------------------------------
 // launches
 // ------------------------------------------------------------------------------------------------
-template <int NC, typename R, int NT, bool U = false>
-bmc_status launch_chain(const ChainArgs& a, const TaylorTable* tt, cudaStream_t st) {
+template <int NC, typename R, int NT, bool U, bool COUNT>
+bmc_status launch_chain_impl(const ChainArgs& a, const TaylorTable* tt, cudaStream_t st) {
     constexpr int kWarps = ChainLaunch<NC, NT>::kWarps;
     const size_t smem = kWarps * sizeof(DenseSmem<NC, typename DenseReal<R>::type, NT>) +
                         32 * kWarps * sizeof(ChainConst<NC, Dn<R, NT>>);
@@ -318,7 +318,7 @@ bmc_status launch_chain(const ChainArgs& a, const TaylorTable* tt, cudaStream_t 
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
     if (dev >= 64 || !((configured.load(std::memory_order_acquire) >> dev) & 1ull)) {
-        CUDA_TRY(cudaFuncSetAttribute(chain_kernel<NC, R, NT, U>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        CUDA_TRY(cudaFuncSetAttribute(chain_kernel<NC, R, NT, U, COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
         if (dev < 64) configured.fetch_or(1ull << dev, std::memory_order_acq_rel);
     }
@@ -328,9 +328,20 @@ bmc_status launch_chain(const ChainArgs& a, const TaylorTable* tt, cudaStream_t 
     if (blocks == 0) return BMC_OK;
     TaylorTable th;
     if (bmc_status s = host_table_of(tt, &th); s != BMC_OK) return s;
-    chain_kernel<NC, R, NT, U><<<(unsigned)blocks, kWarps * 32, smem, st>>>(a, th);
+    chain_kernel<NC, R, NT, U, COUNT><<<(unsigned)blocks, kWarps * 32, smem, st>>>(a, th);
     CUDA_TRY(cudaGetLastError());
     return BMC_OK;
+}
+
+// the counting instantiation only where a.work asks for counts (the uneven plans never do)
+template <int NC, typename R, int NT, bool U = false>
+bmc_status launch_chain(const ChainArgs& a, const TaylorTable* tt, cudaStream_t st) {
+    if constexpr (!U) {
+        if (a.work) return launch_chain_impl<NC, R, NT, U, true>(a, tt, st);
+    } else {
+        if (a.work) return fail(BMC_ERR_UNSUPPORTED, "work counts of an uneven plan");
+    }
+    return launch_chain_impl<NC, R, NT, U, false>(a, tt, st);
 }
 
 // Tangent mode (bmc_set_tangent_mode): BMC_TANGENTS_AUTO takes the adjoint kernel where it applies.
@@ -351,14 +362,16 @@ bmc_status launch_adjoint(const ChainArgs& a, const int* row_ev, int n_tan, cons
     const long long blocks = (nch + kAdjWarps * 32 - 1) / (kAdjWarps * 32);
     if (blocks > 0x7fffffffLL) return fail(BMC_ERR_INVALID, "%lld chains exceed one launch", nch);
     if (blocks == 0) return BMC_OK;
-    adjoint_kernel<NC, kTan><<<(unsigned)blocks, kAdjWarps * 32, smem, st>>>(a, row_ev, n_tan, tt);
+    TaylorTable th;
+    if (bmc_status s = host_table_of(tt, &th); s != BMC_OK) return s;
+    adjoint_kernel<NC, kTan><<<(unsigned)blocks, kAdjWarps * 32, smem, st>>>(a, row_ev, n_tan, th);
     CUDA_TRY(cudaGetLastError());
     return BMC_OK;
 }
 
 template <int NC, bool kTan = true>
 bmc_status launch_adjoint_block(const ChainArgs& a, const int4* blk, int n_tan, const TaylorTable* tt, cudaStream_t st) {
-    const size_t smem = kAdjBlkWarps * DenseGroup<NC>::G * sizeof(AdjBlkSlot<NC>);
+    const size_t smem = kAdjBlkWarps * DenseGroup<NC>::G * sizeof(AdjBlkSlot<NC, kTan>);
     static std::atomic<unsigned long long> configured{0};
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
@@ -370,7 +383,9 @@ bmc_status launch_adjoint_block(const ChainArgs& a, const int4* blk, int n_tan, 
     const long long blocks = (a.n_chains + kAdjBlkWarps * 32 - 1) / (kAdjBlkWarps * 32);
     if (blocks > 0x7fffffffLL) return fail(BMC_ERR_INVALID, "%lld chains exceed one launch", a.n_chains);
     if (blocks == 0) return BMC_OK;
-    adjoint_block_kernel<NC, kTan><<<(unsigned)blocks, kAdjBlkWarps * 32, smem, st>>>(a, blk, n_tan, tt);
+    TaylorTable th;
+    if (bmc_status s = host_table_of(tt, &th); s != BMC_OK) return s;
+    adjoint_block_kernel<NC, kTan><<<(unsigned)blocks, kAdjBlkWarps * 32, smem, st>>>(a, blk, n_tan, th);
     CUDA_TRY(cudaGetLastError());
     return BMC_OK;
 }

@@ -447,7 +447,9 @@ __device__ __forceinline__ void convert_flat(const A& a, B& b) {
 // ------------------------------------------------------------------------------------------------
 // the chain kernel
 // ------------------------------------------------------------------------------------------------
-template <int NC, typename R, int NT, bool UNEVEN = false>
+// COUNT: the launch adds its work counts to a.work (the measurement entry points); the other launches
+// carry no counters at all.
+template <int NC, typename R, int NT, bool UNEVEN = false, bool COUNT = false>
 __global__ void __launch_bounds__(32 * ChainLaunch<NC, NT>::kWarps, ChainLaunch<NC, NT>::kMinBlocks)
 chain_kernel(const ChainArgs a, const __grid_constant__ TaylorTable tt) {
     using D = Dn<R, NT>;
@@ -499,7 +501,7 @@ chain_kernel(const ChainArgs a, const __grid_constant__ TaylorTable tt) {
 
     const size_t ch = UNEVEN ? (size_t)ci : (size_t)v * a.n_off + o;
     unsigned wk0 = 0, wk1 = 0, wk2 = 0, wk3 = 0, wk4 = 0;   // this chain's work counts (each < 2^32 per launch)
-    const bool count = a.work != nullptr;
+    constexpr bool count = COUNT;
     ChainConst<NC, D>& cc =
         reinterpret_cast<ChainConst<NC, D>*>(smem_raw + ChainLaunch<NC, NT>::kWarps * sizeof(SM))[threadIdx.x];
     for (int node = 0; node < a.n_nodes; ++node) {
@@ -653,7 +655,7 @@ chain_kernel(const ChainArgs a, const __grid_constant__ TaylorTable tt) {
             }
         }
     }
-    if (a.work) {
+    if constexpr (COUNT) {
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
             const unsigned wq = q == 0 ? wk0 : (q == 1 ? wk1 : (q == 2 ? wk2 : (q == 3 ? wk3 : wk4)));
