@@ -182,7 +182,8 @@ def _build_direction(build: Callable, d, i: int, h: float, ref):
             raise ValueError(f"build(d) must keep the pools and mz_loc as setting {i} moves")
         pts[k] = ([np.asarray(getattr(ev, f), np.float64) for f in _EV_FIELDS], pack_params(ex.params, 1)[:, 0],
                   np.asarray(ex.m0, np.float64).reshape(-1))
-    st = lambda a2, a1, m1, m2: (-a2 + 8.0 * a1 - 8.0 * m1 + m2) / (12.0 * h)
+    # the differences first: an entry the setting does not move gets exactly zero
+    st = lambda a2, a1, m1, m2: (8.0 * (a1 - m1) - (a2 - m2)) / (12.0 * h)
     ev = [st(pts[2][0][j], pts[1][0][j], pts[-1][0][j], pts[-2][0][j]) for j in range(len(_EV_FIELDS))]
     return ev, st(pts[2][1], pts[1][1], pts[-1][1], pts[-2][1]), st(pts[2][2], pts[1][2], pts[-1][2], pts[-2][2])
 

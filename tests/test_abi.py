@@ -85,3 +85,35 @@ def test_tangent_mode_switch_is_checked():
         settings.use_tangents("reverse")
     assert settings.use_tangents("forward") == "forward" and settings.tangent_mode() == "forward"
     assert settings.use_tangents("auto") == "auto"
+
+
+def test_design_jvp_arguments_are_checked():
+    """bmc_simulate_design_jvp refuses what it does not compute (start-state tangents, a spread-width
+    tangent, float32, a whole-state output) and null outputs, with a status, before touching the GPU."""
+    L = _lib.lib()
+    dummy = C.c_void_p(16)
+    ev = _lib.Events(16, 16, 16, 16, 16, 16)
+    pr = _lib.Problem(2, 3, 2, 1, 4, 1, 0, 0)
+    tg = _lib.Tangents()
+    tg.n_tangents = 1
+    tg.field_row[0] = 3
+    tg.d_seed = 16
+    call = lambda p, t, z=dummy, jz=dummy, dz=dummy, djz=dummy: L.bmc_simulate_design_jvp(
+        p, dummy, ev, dummy, None, None, None, t, z, jz, dz, djz, None)
+    with pytest.raises(RuntimeError, match="null design-derivative output"):
+        _lib.check(call(pr, tg, dz=None))
+    tg.d_dm0 = 16
+    with pytest.raises(RuntimeError, match="start-state tangents"):
+        _lib.check(call(pr, tg))
+    tg.d_dm0 = None
+    tg.field_row[0] = _lib.SEED_SPREAD_SIGMA
+    with pytest.raises(RuntimeError, match="seeds the spread"):
+        _lib.check(call(pr, tg))
+    tg.field_row[0] = 3
+    with pytest.raises(RuntimeError, match="float64 only"):
+        _lib.check(call(_lib.Problem(2, 3, 2, 1, 4, 1, 1, 0), tg))
+    with pytest.raises(RuntimeError, match="mz_loc >= 0"):
+        _lib.check(call(_lib.Problem(2, 3, 2, 1, -1, 1, 0, 0), tg))
+    tg.n_tangents = 0
+    with pytest.raises(RuntimeError, match="tangents: 1"):
+        _lib.check(call(pr, tg))

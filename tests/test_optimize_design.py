@@ -199,3 +199,34 @@ def test_exact_gradient_of_the_amplitude_ladder(cuda):
         gc = (design_cost(build, setup[4], d + e, SIGMA, truths, ("k", "f")) -
               design_cost(build, setup[4], d - e, SIGMA, truths, ("k", "f"))) / (2 * h)
         assert gc == pytest.approx(g[i], rel=1e-5)
+
+
+def test_build_direction_is_exact_for_affine_builds_and_checks_the_table():
+    """The host side of the exact gradient: the five-point stencil of build(d) gives the table's change per
+    unit of a setting exactly (to rounding) for a build affine in it, and refuses a design that changes
+    the table's shape or event types as it moves."""
+    from bmc_b200.design import _build_direction
+    setup = _setup()
+    build = lambda dd: _ladder(setup, dd)
+    d = np.array([0.5, 1.0, 2.0])
+    ev, p_dir, m_dir = _build_direction(build, d, 1, 1e-3, build(d))
+    base = np.asarray(setup[3][1].rf_amp, np.float64)
+    n = base.shape[0]
+    want = np.zeros((3 * n, base.shape[1]))
+    want[n:2 * n] = base                                  # rung 2's amplitude moves with d[1], 1:1
+    np.testing.assert_allclose(ev[1], want, rtol=0, atol=1e-9 * np.abs(base).max())
+    for j in (0, 2, 3):                                   # dt, phase, frequency do not move
+        assert np.abs(ev[j]).max() < 1e-9
+    assert np.abs(p_dir).max() == 0.0 and np.abs(m_dir).max() == 0.0
+
+    def growing(dd):                                      # a setting that adds events: not differentiable
+        ex = build(dd)
+        if dd[0] > 0.5:
+            from bmc_b200.fitting import Experiment
+            from bmc_b200.simulation import SimEvent
+            e = ex.events
+            ev2 = SimEvent(*[np.concatenate([np.asarray(a), np.asarray(a)[:, :1]], axis=1) for a in e])
+            return Experiment(ex.params, ev2, ex.m0, ex.mz_loc)
+        return ex
+    with pytest.raises(ValueError, match="shape and event types"):
+        _build_direction(growing, d, 0, 1e-3, build(d))
