@@ -27,7 +27,7 @@ EXPORTS = ("bmc_abi_version", "bmc_version", "bmc_last_error", "bmc_release", "b
            "bmc_simulate_jvp", "bmc_simulate_design_jvp", "bmc_simulate_trajectory", "bmc_lm_fit", "bmc_normal_blocks",
            "bmc_simulate_counted", "bmc_simulate_jvp_counted", "bmc_probe_fma_peak", "bmc_simulate_noalloc",
            "bmc_mlp_sizes", "bmc_mlp_sync", "bmc_mlp_forward", "bmc_mlp_backward", "bmc_mlp_adam_step",
-           "bmc_mlp_adam_step_dev", "bmc_uneven_create", "bmc_uneven_simulate",
+           "bmc_mlp_adam_step_dev", "bmc_uneven_uses_block_kernel", "bmc_uneven_create", "bmc_uneven_simulate",
            "bmc_uneven_destroy", "bmc_uneven_set_dense_switch", "bmc_normal_segments", "bmc_schur_step", "bmc_schur_eliminate", "bmc_schur_back",
            "bmc_set_tangent_mode")
 
@@ -120,12 +120,13 @@ def lib():
         L.bmc_uneven_simulate.argtypes = [vp, vp, vp, C.POINTER(Spread), C.POINTER(Tangents), vp, vp, vp, vp]
         L.bmc_uneven_destroy.argtypes = [vp]
         L.bmc_uneven_set_dense_switch.argtypes = [vp, C.c_double]
+        L.bmc_uneven_uses_block_kernel.argtypes = [vp, C.POINTER(C.c_int32)]
         L.bmc_normal_segments.argtypes = [C.c_int32, C.c_int32, C.c_int64, vp, vp, vp, vp, vp, vp, vp]
         L.bmc_schur_step.argtypes = [C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, C.c_double, vp, vp, vp, vp, vp]
         L.bmc_schur_eliminate.argtypes = [C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, C.c_double, vp, vp, vp, vp]
         L.bmc_schur_back.argtypes = [C.c_int32, C.c_int32, C.c_int32, vp, C.c_double, vp, vp, vp, vp, vp]
         for f in ("bmc_uneven_create", "bmc_uneven_simulate", "bmc_uneven_destroy", "bmc_uneven_set_dense_switch",
-                  "bmc_normal_segments",
+                  "bmc_uneven_uses_block_kernel", "bmc_normal_segments",
                   "bmc_schur_step", "bmc_schur_eliminate", "bmc_schur_back"):
             getattr(L, f).restype = C.c_int
         sp, i64p = C.POINTER(MlpShape), C.POINTER(C.c_int64)

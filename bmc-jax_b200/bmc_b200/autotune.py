@@ -18,7 +18,7 @@ import numpy as np
 
 from . import _lib
 
-__all__ = ["tune_dense_switch", "apply_tuning", "plan_key"]
+__all__ = ["tune_dense_switch", "apply_tuning", "plan_key", "uses_block_kernel"]
 
 DEFAULT_CANDIDATES = (3.0, 6.0, 12.0, 25.0, 50.0, 100.0)
 
@@ -34,6 +34,15 @@ def plan_key(group) -> str:
 
 def _set(group, norm: float) -> None:
     _lib.check(_lib.lib().bmc_uneven_set_dense_switch(group.plan.plan, float(norm)))
+
+
+def uses_block_kernel(group) -> bool:
+    """True when the group's plan takes the block kernel (every row one repeated block, automatic tangent
+    mode): all its events are then exponentiated densely and the threshold is not consulted."""
+    import ctypes as C
+    out = C.c_int32(0)
+    _lib.check(_lib.lib().bmc_uneven_uses_block_kernel(group.plan.plan, C.byref(out)))
+    return bool(out.value)
 
 
 def _time_pass(group, repeats: int) -> float:
@@ -55,9 +64,14 @@ def tune_dense_switch(batch, candidates: Sequence[float] = DEFAULT_CANDIDATES, r
                       path: Optional[str] = None) -> Dict[str, dict]:
     """For every pool-count group of `batch`, time one forward pass per candidate threshold, set the
     fastest on the group's plan and return {key: {"dense_switch": best, "ms": {candidate: ms}}}; with
-    `path`, merge the choices into that JSON file."""
+    `path`, merge the choices into that JSON file. A group whose plan takes the block kernel
+    (uses_block_kernel) has no threshold to tune: it gets {"dense_switch": None, "block_kernel": True}."""
     out: Dict[str, dict] = {}
     for g in batch.groups:
+        if uses_block_kernel(g):
+            out[plan_key(g)] = {"dense_switch": None, "block_kernel": True, "ms": {}, "voxels": int(len(g.voxels)),
+                                "chains": int(g.n_chains)}
+            continue
         ms = {}
         for c in candidates:
             _set(g, c)
@@ -81,7 +95,7 @@ def apply_tuning(batch, path: str) -> Dict[str, float]:
     done = {}
     for g in batch.groups:
         k = plan_key(g)
-        if k in stored:
+        if k in stored and stored[k].get("dense_switch") is not None:
             _set(g, stored[k]["dense_switch"])
             done[k] = float(stored[k]["dense_switch"])
     return done

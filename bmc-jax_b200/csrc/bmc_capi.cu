@@ -1092,6 +1092,13 @@ bmc_status bmc_uneven_set_dense_switch(void* plan, double norm) {
     return BMC_OK;
 }
 
+bmc_status bmc_uneven_uses_block_kernel(const void* plan, int32_t* out) {
+    if (!plan || !out) return fail(BMC_ERR_INVALID, "uneven: null plan or output");
+    *out = static_cast<const UnevenPlan*>(plan)->adj_ok &&
+           g_tangent_mode.load(std::memory_order_relaxed) == BMC_TANGENTS_AUTO;
+    return BMC_OK;
+}
+
 bmc_status bmc_uneven_destroy(void* plan) {
     UnevenPlan* pl = static_cast<UnevenPlan*>(plan);
     if (!pl) return BMC_OK;

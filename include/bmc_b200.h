@@ -283,6 +283,10 @@ bmc_status bmc_uneven_destroy(void* plan);
  * 0 restores the library's default (100). A tuning knob with no counterpart in the reference: both
  * paths meet the same tolerance, only their speed differs (bmc_b200.autotune measures it per plan). */
 bmc_status bmc_uneven_set_dense_switch(void* plan, double norm);
+/* *out = 1 when this plan's passes take the block kernel in the current tangent mode (every row one
+ * repeated block of at most two events, BMC_TANGENTS_AUTO): its events are then all exponentiated
+ * densely and the threshold above is not consulted; 0 otherwise. Host only, no device work. */
+bmc_status bmc_uneven_uses_block_kernel(const void* plan, int32_t* out);
 
 /*
  * The damped joint step with one value shared by every sample (fitting/joint.py:149-162's

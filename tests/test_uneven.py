@@ -165,10 +165,20 @@ def test_dense_switch_changes_the_path_not_the_result(mixed, tmp_path):
     with pytest.raises(RuntimeError, match="dense-path norm"):
         _lib.check(_lib.lib().bmc_uneven_set_dense_switch(batch.groups[0].plan.plan, -1.0))
     path = tmp_path / "tuning.json"
-    chosen = tune_dense_switch(batch, candidates=(25.0, 100.0), repeats=1, path=str(path))
-    assert set(chosen) == {k for k in chosen} and len(chosen) == len(batch.groups)
-    again = apply_tuning(UnevenBatch(mixed), str(path))
+    from bmc_b200 import settings
+    from bmc_b200.autotune import plan_key, uses_block_kernel
+    settings.use_tangents("forward")              # every plan on the chain kernel: a threshold to tune
+    try:
+        chosen = tune_dense_switch(batch, candidates=(25.0, 100.0), repeats=1, path=str(path))
+        again = apply_tuning(UnevenBatch(mixed), str(path))
+    finally:
+        settings.use_tangents("auto")
+    assert len(chosen) == len(batch.groups) and all(v["dense_switch"] in (25.0, 100.0) for v in chosen.values())
     assert again == {k: v["dense_switch"] for k, v in chosen.items()}
+    # automatic mode: the plans on the block kernel have no threshold and are not timed
+    auto = tune_dense_switch(batch, candidates=(25.0,), repeats=1)
+    for g in batch.groups:
+        assert (auto[plan_key(g)]["dense_switch"] is None) == uses_block_kernel(g)
 
 
 def test_joint_fit_recovers_the_truth(mixed):
