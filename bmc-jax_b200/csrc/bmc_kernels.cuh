@@ -514,10 +514,9 @@ chain_kernel(const ChainArgs a, const __grid_constant__ TaylorTable tt) {
         C::load_m0(a, v, M);
         bool reset_pending = false;
         R gkey = R(NAN);
-        // The Taylor degree of the last event and the range of sub-step norms it covers, (th_lo, th_hi]:
-        // an event whose norm falls in the same range takes the same degree without a table search.
+        // The Taylor degree of the last event: the next event's search starts there (consecutive events
+        // of a chain need similar degrees), a table read or two from the constant bank.
         int m_prev = 1;
-        R th_lo = R(-INFINITY), th_hi = tt.m_max > 1 ? R(tt.theta[1]) : R(INFINITY);
         const R thm = R(tt.theta[tt.m_max]);
         const bool mt_ls = cc.mt_on && cc.ls != 0;
         D gval = dconst<R, NT>(R(0));
@@ -598,13 +597,9 @@ chain_kernel(const ChainArgs a, const __grid_constant__ TaylorTable tt) {
                     // the previous event's degree: consecutive events of a chain need similar degrees, so
                     // this takes a step or two where a search from 1 takes m
                     int m = m_prev;
-                    if (!(per > th_lo && per <= th_hi)) {
-                        while (m < tt.m_max && R(tt.theta[m]) < per) ++m;
-                        while (m > 1 && R(tt.theta[m - 1]) >= per) --m;
-                        m_prev = m;
-                        th_lo = m > 1 ? R(tt.theta[m - 1]) : R(-INFINITY);
-                        th_hi = m < tt.m_max ? R(tt.theta[m]) : R(INFINITY);
-                    }
+                    while (m < tt.m_max && R(tt.theta[m]) < per) ++m;
+                    while (m > 1 && R(tt.theta[m - 1]) >= per) --m;
+                    m_prev = m;
                     m_own = m;
                 }
                 const int ns_w = __reduce_max_sync(kFull, (unsigned)ns_own);
