@@ -195,11 +195,11 @@ def oracle_check(P, M0, ev, n_cest, z_gpu, n_vox=8):
 
 # ------------------------------------------------------------------------------------------------
 # DRAM bytes per chain of chain_kernel from one ncu capture of a 2,048-voxel x 101-offset launch of the
-# default workload (float64: 22.0 MB read + 37.6 MB written; mixed: 22.0 MB + 22.0 MB; almost all of it
+# default workload (float64: 22.0 MB read + 37.6 MB written; mixed: 22.4 MB + 23.9 MB; almost all of it
 # register-spill traffic); it grows with the number of chains a launch runs. Keyed by (CEST pools,
 # precision, pulses).
 NCU_BYTES_PER_CHAIN = {(4, 0, 20): (21.957632e6 + 37.630464e6) / (2048 * 101),
-                       (4, 2, 20): (21.955072e6 + 22.032640e6) / (2048 * 101)}
+                       (4, 2, 20): (22.438656e6 + 23.910656e6) / (2048 * 101)}
 
 
 def run_ours(args, rank, world, local_rank):
