@@ -106,7 +106,7 @@ TaylorTable make_table(double tol, int m_max, double dense_theta, double dense_s
 // The mixed precision's Taylor tolerance and float32 threshold (BMC_MIXED in include/bmc_b200.h); a
 // build may set others with -D for a sweep.
 #ifndef BMC_MIXED_TOL
-#define BMC_MIXED_TOL 1e-9
+#define BMC_MIXED_TOL 1e-8
 #endif
 #ifndef BMC_MIXED_F32
 #define BMC_MIXED_F32 3.0

@@ -57,7 +57,7 @@ typedef enum {
  * propagation, float64 dense path (about 1e-4 in Z over thousands of pulse samples, the level of the
  * reference's own float32 path). BMC_MIXED: the state and the first Taylor term of every sub-step in
  * float64 (more leading terms where their bound exceeds three times the state), every later term formed
- * in float32, and a truncation tolerance of 1e-9 per sub-step: the state itself is never rounded to
+ * in float32, and a truncation tolerance of 1e-8 per sub-step: the state itself is never rounded to
  * float32 (measured: ~4e-10 in Z over the 4,023-event benchmark train). Forward model only; float64
  * dense path. */
 #define BMC_F64 0
