@@ -55,7 +55,7 @@ struct DesignChain {
     using C = Chain<NC, HD, NT>;
     using St = State<NC, D>;
     static constexpr int N = Layout<NC>::N;
-    // entry i of a state in the reference order (water x y z, then each CEST pool, MT z last)
+    // entry i of a state in the reference's order (x of water and of each CEST pool, then y, then z, MT z last)
     static __device__ __forceinline__ D& el(St& s, int i) { return C::at(s, i); }
 
     // entry e of one of the chain's matrices: [e][chain]
